@@ -1,0 +1,334 @@
+"""Benchmark of the RK3 stage on B200: one JSON line per run (rank 0).
+
+Workload (default): the curvilinear shock case — 256 x 128 x 128 cells on the wavy periodic
+mapping, Ma 1.5 round jet, single-species ideal air, plain FP64 — advanced with the fused
+one-launch-per-stage kernel.  A "step" is one SSP-RK3 step (three stages).
+
+  value  Mcell-stage/s with the state resident in HBM, device-timed with CUDA events over K
+         steps (max over ranks; N ranks run N independent replicas: weak scaling)
+  e2e    the same metric through the public host-buffer call (DeviceCase.advance_from_host):
+         every step uploads the ghosted Q and rho_i from pinned memory and downloads them
+  roofline  the fused stage kernel (the only kernel in the timed loop) against the measured
+         HBM copy bandwidth, with B_alg = 8 (41 + 3 Ns + [Ns >= 2] Ns) bytes per cell-stage
+  cpu_baseline  the oracle (C++ FP64 restatement, OpenMP over all host cores) on a bounded
+         sample of the same workload
+
+`--impl reference` times the reference path's CPU implementation instead (the oracle port:
+the reference's RHS exists only as Julia CUDA.jl kernels and Julia is not installed).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "Mcell-stage/s plain FP64 vs batched mixed-prec; p50/p99 step latency at err"
+UNIT = "Mcell-stage/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
+
+
+def _package():
+    if "flame3d_b200" in sys.modules:
+        return sys.modules["flame3d_b200"]
+    pkg = ROOT / "flame3d.jl_b200"
+    spec = importlib.util.spec_from_file_location("flame3d_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["flame3d_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def b_alg(ns: int, precision: int = 0) -> int:
+    """Algorithmic bytes per interior cell-stage of a perfectly fused stage: Q read 7 +
+    metrics 10 + mu, lambda 2 + U read 5 + Un 5 + U write 5 + Q write 7 = 41 words, plus
+    3 Ns (rho_i read, rho_n, rho_i write) and Ns for D when Ns >= 2.  Mixed precision stores
+    Q, mu, lambda, D in 4 bytes."""
+    d = ns if ns >= 2 else 0
+    if precision == 0:
+        return 8 * (41 + 3 * ns + d)
+    return 4 * (7 + 2 + 7 + d) + 8 * (10 + 15 + 3 * ns)
+
+
+WORKLOADS = {
+    "jet256x128x128": dict(kind="jet", nx=256, ny=128, nz=128),
+    "jet128x64x64": dict(kind="jet", nx=128, ny=64, nz=64),
+    "tgv64": dict(kind="tgv", n=64),
+    "mix192_ns9": dict(kind="mixing", n=192, ns=9),
+}
+
+
+def make_case(f3d, name: str, nz_override: int | None = None):
+    w = dict(WORKLOADS[name])
+    kind = w.pop("kind")
+    if kind == "jet":
+        if nz_override:
+            w["nz"] = nz_override
+        return f3d.curvilinear_jet(**w)
+    if kind == "tgv":
+        return f3d.taylor_green(**w)
+    return f3d.mixing_layer(**w)
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons of one GPU every 100 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                   "-lms", "100"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------ CPU side
+def cpu_sample(f3d, workload: str, stages: int):
+    """Times the oracle on a bounded sample of the workload: `stages` RK3 stages on a
+    256 x 128 x 16 slab of the same mapping and flow (1/8 of the cells)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    lib = oracle.load()
+    w = WORKLOADS[workload]
+    nz = 16 if w["kind"] == "jet" else None
+    case = make_case(f3d, workload, nz_override=nz) if nz else make_case(f3d, workload)
+    oc = oracle.OracleCase(case)
+    oc.stage(1)  # warm-up (page faults, thread pool)
+    t0 = time.perf_counter()
+    for s in range(stages):
+        oc.stage(1 + (s % 3))
+    dt = time.perf_counter() - t0
+    value = case.cells * stages / dt / 1e6
+    return value, lib.oracle_num_threads(), case, dt
+
+
+def run_reference(args, f3d):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    lib = oracle.load()
+    w = WORKLOADS[args.workload]
+    nz = 16 if w["kind"] == "jet" else None
+    case = make_case(f3d, args.workload, nz_override=nz) if nz else make_case(f3d, args.workload)
+    oc = oracle.OracleCase(case)
+    for s in range(args.warmup):
+        oc.stage(1 + s % 3)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        oc.stage(1 + s % 3)
+    dt = time.perf_counter() - t0
+    value = case.cells * args.steps / dt / 1e6
+    sample = (f"each step = 1 RK3 stage of the oracle (C++ FP64 restatement of the reference "
+              f"RHS) on a {case.nx}x{case.ny}x{case.nz} slab of the same workload")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "sample_cells": case.cells},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": lib.oracle_num_threads(),
+                            "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ GPU side
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="jet256x128x128", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-stages", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    f3d = _package()
+    if args.impl == "reference":
+        return run_reference(args, f3d)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    prec = 0 if args.precision == "fp64" else 1
+    case = make_case(f3d, args.workload)
+    dc = f3d.solver().DeviceCase(case, device=dev, precision=prec)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        dc.step()
+    barrier()
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    clk = ClockSampler(f"GPU-{uuid}" if uuid else None)
+    clk.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        dc.step()
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stages = 3 * args.steps
+    cells = case.cells
+    value = world * cells * stages / (ms / 1e3) / 1e6
+    kernel_ms = ms / stages  # the fused stage kernel is the only launch in the loop
+
+    # ---- end to end through the host-buffer API (pinned host memory, copies timed)
+    ns = case.ns
+    Qh = torch.from_numpy(case.Q).pin_memory()
+    rh = torch.from_numpy(case.rhoi).pin_memory()
+    Qo = torch.empty_like(Qh).pin_memory()
+    ro = torch.empty_like(rh).pin_memory()
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        dc.advance_from_host(Qh, rh, 1, Qo, ro)
+    barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        dc.advance_from_host(Qh, rh, 1, Qo, ro)
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * cells * 3 * e2e_steps / (ms_e2e / 1e3) / 1e6
+    h2d = (Qh.numel() * Qh.element_size() + rh.numel() * rh.element_size())
+    d2h = (Qo.numel() * Qo.element_size() + ro.numel() * ro.element_size())
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    # ---- roofline of the fused stage kernel
+    peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    balg = b_alg(ns, prec)
+    achieved = balg * cells / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    if TRAFFIC.exists():
+        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}")
+        if tr:
+            traffic = tr.get("bytes_per_launch")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": "measured" if PEAKS.exists() else "fallback",
+            "kernel": "flame::fused::k_stage", "b_alg_bytes_per_cell": balg,
+            "kernel_ms": kernel_ms}
+
+    cpu = None
+    if not args.no_cpu:
+        cv, cores, cc, secs = cpu_sample(f3d, args.workload, args.cpu_stages)
+        cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_stages} RK3 stages of the oracle on a "
+                         f"{cc.nx}x{cc.ny}x{cc.nz} slab of the workload ({secs:.1f} s)"}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if prec == 0 else "f32/f64",
+           "data": "synthetic (seeded jet on the wavy periodic mapping)",
+           "config": {"workload": args.workload, "cells": cells, "species": ns,
+                      "precision": args.precision, "path": "fused one launch per RK3 stage",
+                      "l2": "inputs larger than L2 (state ~%.1f GB per replica)" % (
+                          (35 + 3 * ns) * case.Q[0].size * 8 / 1e9),
+                      "parallelism": f"replicas x{world}"},
+           "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+           "gpu_launches": stages}
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,134 @@
+"""ctypes view of the C ABI in include/flame3d_b200.h and the loader of libflame3d_b200.so.
+
+The structures here are field-for-field copies of the C structs; the function table gives every
+exported entry point its argument types so a wrong call fails in Python, not on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libflame3d_b200.so"
+HEADER = HERE.parent / "include" / "flame3d_b200.h"
+
+FLAME_NG = 4
+FLAME_MAX_NS = 16
+
+ERRORS = {0: "FLAME_OK", 1: "FLAME_EINVAL", 2: "FLAME_ELAUNCH", 3: "FLAME_ETIMEOUT",
+          4: "FLAME_ENONFINITE", 5: "FLAME_EUNSUPPORTED"}
+
+
+class FlameError(RuntimeError):
+    """A libflame3d_b200 call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class FlameGrid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("ng", C.c_int32),
+                ("ns", C.c_int32), ("periodic", C.c_int32)]
+
+
+class FlameThermo(C.Structure):
+    _fields_ = [("Ru", C.c_double), ("min_temp", C.c_double), ("max_temp", C.c_double),
+                ("ns", C.c_int32), ("pad", C.c_int32),
+                ("mw", C.c_double * FLAME_MAX_NS), ("coeffs_sep", C.c_double * FLAME_MAX_NS),
+                ("coeffs_lo", C.c_double * (7 * FLAME_MAX_NS)),
+                ("coeffs_hi", C.c_double * (7 * FLAME_MAX_NS))]
+
+
+class FlameTransport(C.Structure):
+    _fields_ = [("law", C.c_int32), ("pad", C.c_int32), ("mu_ref", C.c_double),
+                ("T_ref", C.c_double), ("exponent", C.c_double), ("Pr", C.c_double),
+                ("lambda_ref", C.c_double), ("D_ref", C.c_double)]
+
+
+METRIC_NAMES = ("dxidx", "dxidy", "dxidz", "detadx", "detady", "detadz",
+                "dzetadx", "dzetady", "dzetadz", "J")
+
+
+class FlameMetrics(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in METRIC_NAMES]
+
+
+class FlameStageBuffers(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("U", "Un", "Q_in", "Q_out", "rhoi_in", "rhoi_out",
+                                          "rhon")]
+
+
+P = C.c_void_p
+G = C.POINTER(FlameGrid)
+S = C.c_void_p  # cudaStream_t
+M = C.POINTER(FlameMetrics)
+TH = C.POINTER(FlameThermo)
+TR = C.POINTER(FlameTransport)
+I = C.c_int
+D = C.c_double
+
+SIGNATURES = {
+    "flame_shockSensor": [G, S, P, P],
+    "flame_fluxSplit": [G, S, P, P, P, P, P, P, P],
+    "flame_split": [G, S, P, P, P, P, P, P, P, P],
+    "flame_WENO_x": [G, S, P, P, P, P, I, P],
+    "flame_WENO_y": [G, S, P, P, P, P, I, P],
+    "flame_WENO_z": [G, S, P, P, P, P, I, P],
+    "flame_viscousFlux_x": [G, S, P, P, M, P, P, P, P],
+    "flame_viscousFlux_y": [G, S, P, P, M, P, P, P, P],
+    "flame_viscousFlux_z": [G, S, P, P, M, P, P, P, P],
+    "flame_specViscousFlux_x": [G, S, P, P, P, M, P, P, TH, P],
+    "flame_specViscousFlux_y": [G, S, P, P, P, M, P, P, TH, P],
+    "flame_specViscousFlux_z": [G, S, P, P, P, M, P, P, TH, P],
+    "flame_div": [G, S, P, P, P, P, P, P, P, D, P, P],
+    "flame_divSpecs": [G, S, P, P, P, P, P, P, P, D, P, P],
+    "flame_linComb": [G, S, P, P, I, D, D, P],
+    "flame_c2Prim": [G, S, P, P, P, TH, P],
+    "flame_prim2c": [G, S, P, P],
+    "flame_mixture": [G, S, P, P, P, P, P, P, TH, TR, P],
+    "flame_fill_periodic": [G, S, P, I],
+    "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
+    "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
+    "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
+    "flame_last_error": [C.c_char_p, C.c_size_t],
+    "flame_version": [],
+}
+
+
+def header_symbols(path: Path = HEADER) -> list[str]:
+    """Every `flame_*` function the public header declares."""
+    text = path.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\bint\s+(flame_\w+)\s*\(", text)))
+
+
+_LIB: C.CDLL | None = None
+
+
+def load_library(path: Path = LIB_PATH) -> C.CDLL:
+    """Loads the in-tree library (built by build.py); raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not path.exists():
+        raise FlameError(1, f"{path} is missing: build it with `python {HERE/'build.py'}`")
+    lib = C.CDLL(str(path))
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+def last_error(lib: C.CDLL) -> str:
+    buf = C.create_string_buffer(512)
+    lib.flame_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(lib: C.CDLL, rc: int) -> None:
+    if rc != 0:
+        raise FlameError(rc, last_error(lib))

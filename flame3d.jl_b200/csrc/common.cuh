@@ -1,0 +1,234 @@
+// common.cuh — shared device helpers for libflame3d_b200 (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+#include "../../include/flame3d_b200.h"
+
+namespace flame {
+
+constexpr double kEps = 2.220446049250313e-16;  // CUDA.eps(Float64), utils.jl:100
+// Scheme constants, run.jl:51-57.
+constexpr double kWenoEps = 1e-26;
+constexpr double kHybrid1 = 1e-3;
+constexpr double kHybrid2 = 0.1;
+constexpr double kUP7_2 = 17.0 / 600, kUP7_3 = -23.0 / 120, kUP7_4 = 22.0 / 30, kUP7_5 = 0.5,
+                 kUP7_6 = -0.075, kUP7_7 = 0.005;  // UP7[1] is 0 (run.jl:57)
+
+// Extents of a ghosted grid; every array index is computed in 64-bit.
+struct Dims {
+    int nx, ny, nz, ng, ns;
+    long long tx, ty, tz, np;
+    __host__ __device__ long long P(long long i, long long j, long long k) const {
+        return i + tx * (j + ty * k);
+    }
+};
+
+inline Dims make_dims(const FlameGrid &g) {
+    Dims d;
+    d.nx = g.nx, d.ny = g.ny, d.nz = g.nz, d.ng = g.ng, d.ns = g.ns;
+    d.tx = g.nx + 2LL * g.ng, d.ty = g.ny + 2LL * g.ng, d.tz = g.nz + 2LL * g.ng;
+    d.np = d.tx * d.ty * d.tz;
+    return d;
+}
+
+__device__ __forceinline__ double jmax(double a, double b) {  // Julia max: NaN-propagating
+    if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000LL);
+    return a > b ? a : b;
+}
+
+__device__ __forceinline__ int64_t tag_at(const int64_t *tag, long long p) {
+    return tag ? tag[p] : 0;
+}
+
+// ------------------------------------------------------------------ NASA-7 thermo (thermo.jl)
+// h_specs, thermo.jl:107-133 (J/kg)
+__device__ __forceinline__ double h_spec(const FlameThermo &th, int n, double T, double T2,
+                                         double T3, double T4, double T5) {
+    const double *lo = th.coeffs_lo + 7 * n;
+    double h;
+    if (T < th.coeffs_sep[n]) {
+        h = lo[0] * T + lo[1] * T2 + lo[2] * T3 + lo[3] * T4 + lo[4] * T5;
+    } else {
+        const double *hc = th.coeffs_hi + 7 * n;
+        h = hc[0] * T + hc[1] * T2 + hc[2] * T3 + hc[3] * T4 + hc[4] * T5 + (hc[5] - lo[5]);
+    }
+    return h * (th.Ru / th.mw[n]);
+}
+
+// cp_specs, thermo.jl:82-104 (dimensionless cp/R)
+__device__ __forceinline__ double cp_spec(const FlameThermo &th, int n, double T, double T2,
+                                          double T3, double T4) {
+    const double *c = (T < th.coeffs_sep[n]) ? th.coeffs_lo + 7 * n : th.coeffs_hi + 7 * n;
+    return c[0] + c[1] * T + c[2] * T2 + c[3] * T3 + c[4] * T4;
+}
+
+// ei_specs, thermo.jl:136-160 (dimensionless e/R)
+__device__ __forceinline__ double ei_spec(const FlameThermo &th, int n, double T, double T2,
+                                          double T3, double T4, double T5) {
+    const double *lo = th.coeffs_lo + 7 * n;
+    if (T < th.coeffs_sep[n])
+        return (lo[0] - 1) * T + lo[1] * T2 + lo[2] * T3 + lo[3] * T4 + lo[4] * T5;
+    const double *hc = th.coeffs_hi + 7 * n;
+    return (hc[0] - 1) * T + hc[1] * T2 + hc[2] * T3 + hc[3] * T4 + hc[4] * T5 + (hc[5] - lo[5]);
+}
+
+// InternalEnergy, thermo.jl:219-228 (J/m^3)
+template <int NS>
+__device__ __forceinline__ double internal_energy(const FlameThermo &th, int ns, double T,
+                                                  const double *rhoi) {
+    double T2 = 0.5 * T * T;
+    double T3 = 2.0 / 3.0 * T2 * T;
+    double T4 = T2 * T2;
+    double T5 = 0.8 * T4 * T;
+    double r = 0;
+    const int n_end = NS > 0 ? NS : ns;
+#pragma unroll
+    for (int n = 0; n < (NS > 0 ? NS : FLAME_MAX_NS); ++n) {
+        if (n >= n_end) break;
+        r += rhoi[n] * ei_spec(th, n, T, T2, T3, T4, T5) / th.mw[n];
+    }
+    return r * th.Ru;
+}
+
+// CV, thermo.jl:194-203 (J/(m^3 K))
+template <int NS>
+__device__ __forceinline__ double heat_cv(const FlameThermo &th, int ns, double T,
+                                          const double *rhoi) {
+    double T2 = T * T, T3 = T2 * T, T4 = T2 * T2;
+    double r = 0;
+    const int n_end = NS > 0 ? NS : ns;
+#pragma unroll
+    for (int n = 0; n < (NS > 0 ? NS : FLAME_MAX_NS); ++n) {
+        if (n >= n_end) break;
+        r += (cp_spec(th, n, T, T2, T3, T4) - 1) * rhoi[n] / th.mw[n];
+    }
+    return r * th.Ru;
+}
+
+// GetT, thermo.jl:231-282: Newton on e(T) with ±100 K step clamp and break-before-update.
+template <int NS>
+__device__ double get_T(const FlameThermo &th, int ns, double ein, const double *rhoi) {
+    const double tol = 1e-3;
+    const double tmin = th.min_temp, tmax = th.max_temp;
+    const int n_end = NS > 0 ? NS : ns;
+    double emin = internal_energy<NS>(th, ns, tmin, rhoi);
+    double emax = internal_energy<NS>(th, ns, tmax, rhoi);
+    if (ein < emin) return tmin - (emin - ein) / heat_cv<NS>(th, ns, tmin, rhoi);
+    if (ein > emax) return tmax - (emax - ein) / heat_cv<NS>(th, ns, tmax, rhoi);
+    double As = 0;
+    for (int n = 0; n < n_end; ++n) As += (th.coeffs_lo[7 * n] - 1) * th.Ru / th.mw[n] * rhoi[n];
+    double t1 = ein / As;
+    if (t1 < tmin || t1 > tmax) t1 = tmin + (tmax - tmin) / (emax - emin) * (ein - emin);
+    for (int it = 0; it < 30; ++it) {
+        double e1 = internal_energy<NS>(th, ns, t1, rhoi);
+        double cv = heat_cv<NS>(th, ns, t1, rhoi);
+        double dt = (ein - e1) / cv;
+        if (dt > 100.0)
+            dt = 100.0;
+        else if (dt < -100.0)
+            dt = -100.0;
+        else if (fabs(dt) < tol)
+            break;
+        else if (t1 + dt == t1)
+            break;
+        t1 += dt;
+    }
+    return t1;
+}
+
+// Pmixture, thermo.jl:20-26
+template <int NS>
+__device__ __forceinline__ double p_mixture(const FlameThermo &th, int ns, double T,
+                                            const double *rhoi) {
+    double yow = 0;
+    const int n_end = NS > 0 ? NS : ns;
+#pragma unroll
+    for (int n = 0; n < (NS > 0 ? NS : FLAME_MAX_NS); ++n) {
+        if (n >= n_end) break;
+        yow += rhoi[n] / th.mw[n];
+    }
+    return th.Ru * T * yow;
+}
+
+// ----------------------------------------------------------- hybrid reconstruction (schemes.jl)
+template <typename T>
+__device__ __forceinline__ T minmod(T a, T b) {  // schemes.jl:26-28
+    return (a * b > 0) ? ((fabs(a) > fabs(b)) ? b : a) : T(0);
+}
+
+// WENO-Z5 positive-flux reconstruction from V1..V5 = F+[c-3..c+1], schemes.jl:139-162
+template <typename T>
+__device__ __forceinline__ T wenoz_plus(T V1, T V2, T V3, T V4, T V5) {
+    const T tmp1 = T(13.0 / 12.0), tmp2 = T(1.0 / 6.0), q4 = T(0.25), eps = T(kWenoEps);
+    T a, b;
+    a = V1 - 2 * V2 + V3, b = V1 - 4 * V2 + 3 * V3;
+    T s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V2 - V4;
+    T s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V4 + V5, b = 3 * V3 - 4 * V4 + V5;
+    T s33 = tmp1 * (a * a) + q4 * (b * b);
+    T tau = fabs(s11 - s33);
+    T q;
+    q = tau / (eps + s11), s11 = (1 + q * q) * 1;
+    q = tau / (eps + s22), s22 = (1 + q * q) * 6;
+    q = tau / (eps + s33), s33 = (1 + q * q) * 3;
+    T invsum = 1 / (s11 + s22 + s33);
+    T v1 = 2 * V1 - 7 * V2 + 11 * V3;
+    T v2 = -V2 + 5 * V3 + 2 * V4;
+    T v3 = 2 * V3 + 5 * V4 - V5;
+    return tmp2 * invsum * (s11 * v1 + s22 * v2 + s33 * v3);
+}
+
+// WENO-Z5 negative-flux reconstruction from V1..V5 = F-[c-2..c+2], schemes.jl:164-187
+template <typename T>
+__device__ __forceinline__ T wenoz_minus(T V1, T V2, T V3, T V4, T V5) {
+    const T tmp1 = T(13.0 / 12.0), tmp2 = T(1.0 / 6.0), q4 = T(0.25), eps = T(kWenoEps);
+    T a, b;
+    a = V5 - 2 * V4 + V3, b = V5 - 4 * V4 + 3 * V3;
+    T s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V4 - V2;
+    T s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V2 + V1, b = 3 * V3 - 4 * V2 + V1;
+    T s33 = tmp1 * (a * a) + q4 * (b * b);
+    T tau = fabs(s11 - s33);
+    T q;
+    q = tau / (eps + s11), s11 = (1 + q * q) * 1;
+    q = tau / (eps + s22), s22 = (1 + q * q) * 6;
+    q = tau / (eps + s33), s33 = (1 + q * q) * 3;
+    T invsum = 1 / (s11 + s22 + s33);
+    T v1 = 11 * V3 - 7 * V4 + 2 * V5;
+    T v2 = -V4 + 5 * V3 + 2 * V2;
+    T v3 = 2 * V3 + 5 * V2 - V1;
+    return tmp2 * invsum * (s11 * v1 + s22 * v2 + s33 * v3);
+}
+
+// One face of the hybrid scheme, schemes.jl:110-199.  p[0..6] = F+[c-3..c+3] (F+[c-4] has
+// weight UP7[1] = 0 and is not read), m[0..6] = F-[c-3..c+3]; the face lies between c-1 and c.
+template <typename T>
+__device__ __forceinline__ T hybrid_face7(const T *p, const T *m, T phif) {
+    T fp, fm;
+    if (phif < T(kHybrid1)) {
+        fp = T(kUP7_2) * p[0] + T(kUP7_3) * p[1] + T(kUP7_4) * p[2] + T(kUP7_5) * p[3] +
+             T(kUP7_6) * p[4] + T(kUP7_7) * p[5];
+        fm = T(kUP7_7) * m[0] + T(kUP7_6) * m[1] + T(kUP7_5) * m[2] + T(kUP7_4) * m[3] +
+             T(kUP7_3) * m[4] + T(kUP7_2) * m[5];
+    } else if (phif < T(kHybrid2)) {
+        fp = wenoz_plus(p[0], p[1], p[2], p[3], p[4]);
+        fm = wenoz_minus(m[1], m[2], m[3], m[4], m[5]);
+    } else {
+        fp = p[2] + T(0.5) * minmod(p[3] - p[2], p[2] - p[1]);
+        fm = m[3] - T(0.5) * minmod(m[4] - m[3], m[3] - m[2]);
+    }
+    return fp + fm;
+}
+
+}  // namespace flame
+
+// Error plumbing shared by every C entry point (defined in capi.cu).
+int flame_fail(int code, const char *fmt, ...);
+int flame_check_launch(const char *what);
+int flame_check_grid(const FlameGrid *g, const char *what);

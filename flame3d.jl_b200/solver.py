@@ -1,0 +1,173 @@
+"""Host-side mirror of solver.jl's stage loop over the libflame3d_b200 C ABI.
+
+`DeviceCase` keeps one case's state and metrics resident on a GPU (torch tensors are only the
+allocator and the stream; every computation is a call into the sm_100a library):
+
+  * `stage_sequence(s)` issues the reference's own launch sequence for one RK3 stage
+    (solver.jl:298-326: mixture, shockSensor, specAdvance, flowAdvance, linComb, c2Prim and the
+    ghost fill) through the 1:1 entry points;
+  * `stage_fused(s)` is the same stage as one `flame_rk_stage` launch.
+
+Both take the primitive state Q, rho_i (ghosts filled) to the next stage's Q, rho_i.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from .abi import FlameMetrics, FlameStageBuffers, METRIC_NAMES
+from .cases import Case
+
+RK3 = {2: (0.25, 0.75), 3: (2.0 / 3.0, 1.0 / 3.0)}
+
+
+def _p(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+class DeviceCase:
+    """One case resident on one GPU."""
+
+    def __init__(self, case: Case, device: str | torch.device = "cuda", precision: int = 0,
+                 sequence_buffers: bool = False):
+        self.lib = abi.load_library()
+        self.case = case
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise abi.FlameError(1, "DeviceCase needs a CUDA device; there is no CPU path")
+        self.precision = precision
+        self.grid = case.grid()
+        self.thermo = case.thermo.to_c()
+        self.transport = case.transport.to_c()
+        self.dt = case.dt
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        qdt = torch.float64 if precision == 0 else torch.float32
+
+        def up(a, dtype=torch.float64):
+            return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dtype)
+
+        self.metrics = {k: up(case.metrics[k]) for k in METRIC_NAMES}
+        self.cmetrics = FlameMetrics(**{k: v.data_ptr() for k, v in self.metrics.items()})
+        shp = case.Q.shape[1:]
+        ns = case.ns
+        self.Q = [up(case.Q, qdt), torch.empty((7,) + shp, dtype=qdt, device=dev)]
+        self.rhoi = [up(case.rhoi), torch.empty((ns,) + shp, **f64)]
+        self.Q[1].copy_(self.Q[0])
+        self.rhoi[1].copy_(self.rhoi[0])
+        self.cur = 0
+        self.U = torch.empty((5,) + shp, **f64)
+        self.Un = torch.empty((5,) + shp, **f64)
+        self.rhon = torch.empty((ns,) + shp, **f64)
+        if precision == 0:
+            self._call("flame_prim2c", _p(self.U), _p(self.Q[0]))
+        else:
+            self.U.copy_(torch.from_numpy(case.U()).to(dev))
+        self.seq = None
+        if sequence_buffers:
+            self._alloc_sequence()
+
+    # ------------------------------------------------------------------ plumbing
+    @property
+    def stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _call(self, name: str, *args):
+        fn = getattr(self.lib, name)
+        rc = fn(C.byref(self.grid), C.c_void_p(self.stream), *args)
+        abi.check(self.lib, rc)
+
+    def _alloc_sequence(self):
+        c = self.case
+        shp = c.Q.shape[1:]
+        ns = c.ns
+        nx, ny, nz = c.nx, c.ny, c.nz
+        f64 = dict(dtype=torch.float64, device=self.device)
+        fx, fy, fz = (nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx)
+        z = torch.zeros
+        self.seq = dict(
+            Yi=z((ns,) + shp, **f64), lam=z(shp, **f64), mu=z(shp, **f64), D=z((ns,) + shp, **f64),
+            phi=z(shp, **f64), Fp=z((5,) + shp, **f64), Fm=z((5,) + shp, **f64),
+            Fpi=z((ns,) + shp, **f64), Fmi=z((ns,) + shp, **f64),
+            Fx=z((5,) + fx, **f64), Fy=z((5,) + fy, **f64), Fz=z((5,) + fz, **f64),
+            Fvx=z((4,) + fx, **f64), Fvy=z((4,) + fy, **f64), Fvz=z((4,) + fz, **f64),
+            Fxi=z((ns,) + fx, **f64), Fyi=z((ns,) + fy, **f64), Fzi=z((ns,) + fz, **f64),
+            Fdx=z((ns,) + fx, **f64), Fdy=z((ns,) + fy, **f64), Fdz=z((ns,) + fz, **f64),
+            Fhx=z((3,) + fx, **f64), Fhy=z((3,) + fy, **f64), Fhz=z((3,) + fz, **f64),
+        )
+
+    # ------------------------------------------------------------------ stages
+    def stage_sequence(self, stage: int) -> None:
+        """solver.jl:298-326 through the 1:1 entry points (plain FP64 only)."""
+        if self.precision != 0:
+            raise abi.FlameError(5, "the launch sequence is FP64 only")
+        if self.seq is None:
+            self._alloc_sequence()
+        w = self.seq
+        Q, ri = self.Q[self.cur], self.rhoi[self.cur]
+        g = C.byref
+        dt = C.c_double(self.dt)
+        if stage == 1:
+            self.Un.copy_(self.U)
+            self.rhon.copy_(ri)
+        self._call("flame_mixture", _p(Q), _p(ri), _p(w["Yi"]), _p(w["lam"]), _p(w["mu"]),
+                   _p(w["D"]), g(self.thermo), g(self.transport), None)
+        self._call("flame_shockSensor", _p(w["phi"]), _p(Q))
+        self._call("flame_specAdvance", _p(ri), _p(Q), _p(w["Yi"]), _p(w["Fpi"]), _p(w["Fmi"]),
+                   _p(w["Fxi"]), _p(w["Fyi"]), _p(w["Fzi"]), _p(w["Fdx"]), _p(w["Fdy"]),
+                   _p(w["Fdz"]), g(self.cmetrics), dt, _p(w["phi"]), _p(w["D"]), _p(w["Fhx"]),
+                   _p(w["Fhy"]), _p(w["Fhz"]), g(self.thermo), None)
+        self._call("flame_flowAdvance", _p(self.U), _p(Q), _p(w["Fp"]), _p(w["Fm"]), _p(w["Fx"]),
+                   _p(w["Fy"]), _p(w["Fz"]), _p(w["Fvx"]), _p(w["Fvy"]), _p(w["Fvz"]),
+                   g(self.cmetrics), dt, _p(w["phi"]), _p(w["lam"]), _p(w["mu"]), _p(w["Fhx"]),
+                   _p(w["Fhy"]), _p(w["Fhz"]), None)
+        if stage in RK3:
+            a, b = RK3[stage]
+            self._call("flame_linComb", _p(self.U), _p(self.Un), 5, a, b, None)
+            self._call("flame_linComb", _p(ri), _p(self.rhon), self.case.ns, a, b, None)
+        self._call("flame_c2Prim", _p(self.U), _p(Q), _p(ri), g(self.thermo), None)
+        self._call("flame_fill_periodic", _p(Q), 7)
+        self._call("flame_fill_periodic", _p(ri), self.case.ns)
+
+    def stage_fused(self, stage: int) -> None:
+        """The same stage as one flame_rk_stage launch (ping-pong of Q and rho_i)."""
+        i, o = self.cur, 1 - self.cur
+        b = FlameStageBuffers(_p(self.U), _p(self.Un), _p(self.Q[i]), _p(self.Q[o]),
+                              _p(self.rhoi[i]), _p(self.rhoi[o]), _p(self.rhon))
+        rc = self.lib.flame_rk_stage(C.byref(self.grid), C.c_void_p(self.stream), stage,
+                                     self.dt, C.byref(b), C.byref(self.cmetrics),
+                                     C.byref(self.thermo), C.byref(self.transport),
+                                     self.precision)
+        abi.check(self.lib, rc)
+        self.cur = o
+
+    def step(self, fused: bool = True) -> None:
+        for s in (1, 2, 3):
+            (self.stage_fused if fused else self.stage_sequence)(s)
+
+    def advance_from_host(self, Q_host: torch.Tensor, rhoi_host: torch.Tensor, nsteps: int,
+                          Q_out: torch.Tensor, rhoi_out: torch.Tensor) -> None:
+        """End-to-end call with host buffers: uploads the primitive state (ghosted Q, rho_i,
+        ideally pinned), rebuilds U (prim2c, utils.jl:71-92), advances `nsteps` RK3 steps with
+        the fused stage and downloads the resulting Q, rho_i.  Asynchronous on the current
+        stream; synchronize before reading the outputs."""
+        if self.precision != 0:
+            raise abi.FlameError(5, "advance_from_host is implemented for the FP64 path")
+        Q, r = self.Q[self.cur], self.rhoi[self.cur]
+        Q.copy_(Q_host, non_blocking=True)
+        r.copy_(rhoi_host, non_blocking=True)
+        self._call("flame_prim2c", _p(self.U), _p(Q))
+        for _ in range(nsteps):
+            self.step()
+        Q_out.copy_(self.Q[self.cur], non_blocking=True)
+        rhoi_out.copy_(self.rhoi[self.cur], non_blocking=True)
+
+    # ------------------------------------------------------------------ results
+    def primitives(self) -> tuple[np.ndarray, np.ndarray]:
+        return (self.Q[self.cur].double().cpu().numpy(), self.rhoi[self.cur].cpu().numpy())
+
+    def conserved(self) -> np.ndarray:
+        return self.U.cpu().numpy()

@@ -1,0 +1,217 @@
+/*
+ * flame3d_b200.h — C ABI of libflame3d_b200.so, the sm_100a (B200) implementation of
+ * Flame3D.jl's per-stage right-hand side on curvilinear grids and its SSP-RK3 stage update.
+ *
+ * Conventions (shared by every entry point):
+ *   - Arrays are the reference's Julia arrays, column-major with i fastest, SoA by variable:
+ *     ghosted point (i, j, k, n), 0-based, lives at  i + Tx*(j + Ty*(k + Tz*n))  with
+ *     Tx = nx + 2*ng, Ty = ny + 2*ng, Tz = nz + 2*ng.  Face arrays are unghosted with one extra
+ *     face along the swept axis: an x-face array is (nx+1, ny, nz, NV), face f lies between
+ *     ghosted cells ng+f-1 and ng+f.  Same shapes as solver.jl:141-167.
+ *   - All floating point arrays are FP64 device pointers owned by the caller (Julia CuArray or
+ *     torch tensor); the library only borrows them for the duration of the (asynchronous) call.
+ *   - `tag` is the IBM tag field (Int64, solver.jl:123).  NULL means "all fluid" (tag == 0),
+ *     which is the only value the fused entry points accept.
+ *   - Every call is asynchronous on `stream` (NULL = legacy default stream) and returns
+ *     FLAME_OK or an error code; flame_last_error() gives the message of the calling thread.
+ *   - The library keeps no global mutable state besides a per-thread error string.
+ *
+ * The argument order after (grid, stream) is the argument order of the reference kernel each
+ * entry point replaces, so a Julia `ccall` is a mechanical rewrite of the `@cuda` launch.
+ */
+#ifndef FLAME3D_B200_H
+#define FLAME3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *flame_stream_t; /* identical to cudaStream_t */
+
+#define FLAME_NG 4      /* ghost layers; parse_mesh.jl:5 */
+#define FLAME_MAX_NS 16 /* largest species count compiled in */
+
+enum {
+    FLAME_OK = 0,
+    FLAME_EINVAL = 1,      /* bad argument (NULL pointer, size, ng != 4, ns out of range) */
+    FLAME_ELAUNCH = 2,     /* CUDA reported an error at launch */
+    FLAME_ETIMEOUT = 3,    /* a bounded device wait gave up */
+    FLAME_ENONFINITE = 4,  /* a non-finite conserved value was detected */
+    FLAME_EUNSUPPORTED = 5 /* valid request this build does not implement */
+};
+
+/* Grid extents; the reference keeps these as compile-time constants (run.jl:59-63). */
+typedef struct FlameGrid {
+    int32_t nx, ny, nz; /* interior cells (Nxp, Ny, Nz) */
+    int32_t ng;         /* ghost layers, must be FLAME_NG */
+    int32_t ns;         /* species count (Nspecs), 1..FLAME_MAX_NS */
+    int32_t periodic;   /* bit 0/1/2: x/y/z periodic (ghost fill and fused stage) */
+} FlameGrid;
+
+/* NASA-7 thermodynamics; the by-value counterpart of thermoProperty (run.jl:71-82).
+ * coeffs_lo / coeffs_hi are the Julia (7, ns) matrices, column-major: [a + 7*n]. */
+typedef struct FlameThermo {
+    double Ru;       /* J/(mol K) */
+    double min_temp; /* K */
+    double max_temp; /* K */
+    int32_t ns;
+    int32_t pad;
+    double mw[FLAME_MAX_NS];         /* kg/mol */
+    double coeffs_sep[FLAME_MAX_NS]; /* K, switch between the low and high range */
+    double coeffs_lo[7 * FLAME_MAX_NS];
+    double coeffs_hi[7 * FLAME_MAX_NS];
+} FlameThermo;
+
+/* Transport law that stands in for Cantera's mixture-averaged fits (thermo.jl:289-403).
+ *   law 0: mu = mu_ref, lambda = lambda_ref, D_k = D_ref (constants)
+ *   law 1: mu = mu_ref * (T / T_ref)^exponent, lambda = cp * mu / Pr with cp the mass-specific
+ *          mixture heat capacity, D_k = lambda / (rho * cp) for every species (unity Lewis). */
+typedef struct FlameTransport {
+    int32_t law;
+    int32_t pad;
+    double mu_ref, T_ref, exponent, Pr, lambda_ref, D_ref;
+} FlameTransport;
+
+/* Curvilinear metrics (J^-1-scaled cofactors, parse_mesh.jl:210-221) and J, all ghosted. */
+typedef struct FlameMetrics {
+    const double *dxidx, *dxidy, *dxidz;
+    const double *detadx, *detady, *detadz;
+    const double *dzetadx, *dzetady, *dzetadz;
+    const double *J;
+} FlameMetrics;
+
+/* ---------------------------------------------------------------------------------------
+ * 1:1 replacements of the reference kernels (same index ranges, same arithmetic).
+ * ------------------------------------------------------------------------------------- */
+
+/* schemes.jl:1-24  shockSensor(ϕ, Q) */
+int flame_shockSensor(const FlameGrid *g, flame_stream_t stream, double *phi, const double *Q);
+
+/* split.jl:17-89  fluxSplit(Q, Fp, Fm, Ax, Ay, Az, tag); Fp/Fm are ghosted (…, 5) */
+int flame_fluxSplit(const FlameGrid *g, flame_stream_t stream, const double *Q, double *Fp,
+                    double *Fm, const double *Ax, const double *Ay, const double *Az,
+                    const int64_t *tag);
+
+/* split.jl:101-130  split(ρi, Q, Fp, Fm, Ax, Ay, Az, tag); Fp/Fm are ghosted (…, ns) */
+int flame_split(const FlameGrid *g, flame_stream_t stream, const double *rhoi, const double *Q,
+                double *Fp, double *Fm, const double *Ax, const double *Ay, const double *Az,
+                const int64_t *tag);
+
+/* schemes.jl:86-437  WENO_x/y/z(F, ϕ, Fp, Fm, NV, tag): hybrid UP7 / WENO-Z5 / minmod */
+int flame_WENO_x(const FlameGrid *g, flame_stream_t stream, double *F, const double *phi,
+                 const double *Fp, const double *Fm, int NV, const int64_t *tag);
+int flame_WENO_y(const FlameGrid *g, flame_stream_t stream, double *F, const double *phi,
+                 const double *Fp, const double *Fm, int NV, const int64_t *tag);
+int flame_WENO_z(const FlameGrid *g, flame_stream_t stream, double *F, const double *phi,
+                 const double *Fp, const double *Fm, int NV, const int64_t *tag);
+
+/* viscous.jl:1-428  viscousFlux_x/y/z(Fv, Q, 9 metrics, J, λ, μ, Fh, tag); Fv is (faces, 4) */
+int flame_viscousFlux_x(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
+                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *Fh, const int64_t *tag);
+int flame_viscousFlux_y(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
+                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *Fh, const int64_t *tag);
+int flame_viscousFlux_z(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
+                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *Fh, const int64_t *tag);
+
+/* viscous.jl:430-665  specViscousFlux_x/y/z(Fd, Q, Yi, 9 metrics, J, D, Fh, thermo, tag);
+ * Fd is (faces, ns), Fh (faces, 3) is written. */
+int flame_specViscousFlux_x(const FlameGrid *g, flame_stream_t stream, double *Fd,
+                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *D, double *Fh, const FlameThermo *thermo,
+                            const int64_t *tag);
+int flame_specViscousFlux_y(const FlameGrid *g, flame_stream_t stream, double *Fd,
+                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *D, double *Fh, const FlameThermo *thermo,
+                            const int64_t *tag);
+int flame_specViscousFlux_z(const FlameGrid *g, flame_stream_t stream, double *Fd,
+                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *D, double *Fh, const FlameThermo *thermo,
+                            const int64_t *tag);
+
+/* div.jl:16-54  div(U, Fx, Fy, Fz, Fv_x, Fv_y, Fv_z, dt, J, tag): U += J dt (−ΔF + ΔFv) */
+int flame_div(const FlameGrid *g, flame_stream_t stream, double *U, const double *Fx,
+              const double *Fy, const double *Fz, const double *Fv_x, const double *Fv_y,
+              const double *Fv_z, double dt, const double *J, const int64_t *tag);
+
+/* div.jl:61-84  divSpecs(ρi, Fx, Fy, Fz, Fd_x, Fd_y, Fd_z, dt, J, tag) */
+int flame_divSpecs(const FlameGrid *g, flame_stream_t stream, double *rhoi, const double *Fx,
+                   const double *Fy, const double *Fz, const double *Fd_x, const double *Fd_y,
+                   const double *Fd_z, double dt, const double *J, const int64_t *tag);
+
+/* utils.jl:95-112  linComb(U, Un, NV, a, b, tag): U = a U + b Un on interior points */
+int flame_linComb(const FlameGrid *g, flame_stream_t stream, double *U, const double *Un,
+                  int NV, double a, double b, const int64_t *tag);
+
+/* utils.jl:2-48 (+ thermo.jl:231-282 GetT)  c2Prim(U, Q, ρi, thermo, tag) */
+int flame_c2Prim(const FlameGrid *g, flame_stream_t stream, const double *U, double *Q,
+                 double *rhoi, const FlameThermo *thermo, const int64_t *tag);
+
+/* utils.jl:71-92  prim2c(U, Q) over all ghosted points */
+int flame_prim2c(const FlameGrid *g, flame_stream_t stream, double *U, const double *Q);
+
+/* thermo.jl:371-403  mixture(Q, ρi, Yi, λ, μ, D, thermo, tag) with the FlameTransport law in
+ * place of Cantera's fits; Yi = max(ρi / max(ρ, eps), 0) exactly as the reference. */
+int flame_mixture(const FlameGrid *g, flame_stream_t stream, const double *Q, const double *rhoi,
+                  double *Yi, double *lambda, double *mu, double *D, const FlameThermo *thermo,
+                  const FlameTransport *transport, const int64_t *tag);
+
+/* Periodic ghost fill of `nv` ghosted fields (new: the reference's fills, boundary.jl:1-191,
+ * are case-specific inflow / zero-gradient; all benchmark cases are periodic). */
+int flame_fill_periodic(const FlameGrid *g, flame_stream_t stream, double *A, int nv);
+
+/* solver.jl:22-38  flowAdvance(…): fluxSplit+WENO per direction, viscousFlux ×3, div.
+ * Fp/Fm are ghosted (…,5) scratch; Fx/Fy/Fz face (…,5); Fv_* face (…,4); Fh* face (…,3). */
+int flame_flowAdvance(const FlameGrid *g, flame_stream_t stream, double *U, const double *Q,
+                      double *Fp, double *Fm, double *Fx, double *Fy, double *Fz, double *Fv_x,
+                      double *Fv_y, double *Fv_z, const FlameMetrics *m, double dt,
+                      const double *phi, const double *lambda, const double *mu,
+                      const double *Fhx, const double *Fhy, const double *Fhz,
+                      const int64_t *tag);
+
+/* solver.jl:40-56  specAdvance(…): split+WENO per direction, specViscousFlux ×3, divSpecs. */
+int flame_specAdvance(const FlameGrid *g, flame_stream_t stream, double *rhoi, const double *Q,
+                      const double *Yi, double *Fp_i, double *Fm_i, double *Fx_i, double *Fy_i,
+                      double *Fz_i, double *Fd_x, double *Fd_y, double *Fd_z,
+                      const FlameMetrics *m, double dt, const double *phi, const double *D,
+                      double *Fhx, double *Fhy, double *Fhz, const FlameThermo *thermo,
+                      const int64_t *tag);
+
+/* ---------------------------------------------------------------------------------------
+ * Fused path: one launch per RK3 stage (solver.jl:297-326 for periodic grids, IBM off).
+ * Reads Q_in / rhoi_in (ghosts filled), writes U in place, Q_out / rhoi_out including their
+ * periodic ghost images, so the caller swaps the in/out pair after every stage.
+ * Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
+ * ------------------------------------------------------------------------------------- */
+typedef struct FlameStageBuffers {
+    double *U;             /* (…,5) conserved, interior updated in place */
+    double *Un;            /* (…,5) RK3 stage-0 copy */
+    const double *Q_in;    /* (…,7) primitives of the stage input, ghosts filled */
+    double *Q_out;         /* (…,7) primitives of the stage result, ghosts filled */
+    const double *rhoi_in; /* (…,ns) partial densities of the stage input, ghosts filled */
+    double *rhoi_out;      /* (…,ns) partial densities of the stage result, ghosts filled */
+    double *rhon;          /* (…,ns) RK3 stage-0 copy */
+} FlameStageBuffers;
+
+/* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 split/recon/viscous,
+ * FP64 accumulation, metrics and Newton temperature). */
+int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
+                   const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *thermo,
+                   const FlameTransport *transport, int precision);
+
+/* Message of the last error on the calling thread; returns its length. */
+int flame_last_error(char *buf, size_t n);
+
+/* ABI version (major*10000 + minor*100 + patch). */
+int flame_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLAME3D_B200_H */
