@@ -203,6 +203,8 @@ def main() -> int:
     ap.add_argument("--workload", default="jet256x128x128", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-stages", type=int, default=3)
+    ap.add_argument("--tile", type=int, default=None,
+                    help="stage configuration (0-3); default: the autotuner's choice")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -224,7 +226,7 @@ def main() -> int:
                                 device_id=dev)
     prec = 0 if args.precision == "fp64" else 1
     case = make_case(f3d, args.workload)
-    dc = f3d.solver().DeviceCase(case, device=dev, precision=prec)
+    dc = f3d.solver_module().DeviceCase(case, device=dev, precision=prec, tile=args.tile)
     stream = torch.cuda.current_stream(dev)
 
     def barrier():

@@ -16,7 +16,7 @@ __all__ = ["FlameError", "FlameGrid", "FlameMetrics", "FlameStageBuffers", "Flam
            "ideal_air", "synthetic_species"]
 
 
-def solver():
+def solver_module():
     """The torch-backed solver module (imported lazily so `import flame3d_b200` stays light)."""
-    from . import solver as _s
-    return _s
+    import importlib
+    return importlib.import_module(__name__ + ".solver")

@@ -57,7 +57,7 @@ class FlameMetrics(C.Structure):
 
 class FlameStageBuffers(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("U", "Un", "Q_in", "Q_out", "rhoi_in", "rhoi_out",
-                                          "rhon")]
+                                          "rhon", "trans_in", "trans_out", "scratch")]
 
 
 P = C.c_void_p
@@ -92,6 +92,9 @@ SIGNATURES = {
     "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
     "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
+    "flame_rk_stage_tiled": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I, I],
+    "flame_transport": [G, S, P, P, P, TH, TR, I],
+    "flame_stage_scratch_bytes": [G, I],
     "flame_last_error": [C.c_char_p, C.c_size_t],
     "flame_version": [],
 }
@@ -101,7 +104,7 @@ def header_symbols(path: Path = HEADER) -> list[str]:
     """Every `flame_*` function the public header declares."""
     text = path.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\bint\s+(flame_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(?:int|size_t)\s+(flame_\w+)\s*\(", text)))
 
 
 _LIB: C.CDLL | None = None
@@ -118,7 +121,7 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = C.c_int
+        fn.restype = C.c_size_t if name == "flame_stage_scratch_bytes" else C.c_int
     _LIB = lib
     return lib
 

@@ -418,9 +418,12 @@ def random_curvilinear(n: int = 16, ns: int = 1, seed: int = 11, amp: float = 0.
     tp = 2 * math.pi
     T = T_range[0] + (T_range[1] - T_range[0]) * (0.5 + 0.4 * np.sin(tp * X) * np.cos(tp * Y))
     T *= 1 + 0.05 * rng.uniform(-1, 1, T.shape)
-    p = 1e5 * (1 + 0.3 * np.sin(tp * Z) + noise * rng.uniform(-1, 1, T.shape))
-    # a few strong pressure jumps put faces in the minmod branch
-    p[:, :, nx // 2:] *= 1.6
+    # smooth pressure in the first third of x (UP7 faces), noise in the middle third (WENO-Z)
+    # and a 1.6x jump at two thirds (minmod faces)
+    p = 1e5 * (1 + 0.3 * np.sin(tp * Z))
+    mid = (ii >= nx // 3) & (ii < 2 * nx // 3)
+    p = p * (1 + noise * rng.uniform(-1, 1, T.shape) * mid)
+    p[:, :, 2 * nx // 3:] *= 1.6
     Ys = rng.dirichlet(np.ones(ns), size=T.shape).transpose(3, 0, 1, 2) if ns > 1 \
         else np.ones((1,) + T.shape)
     Wmix = 1.0 / np.sum(Ys / thermo.mw[:, None, None, None], axis=0)

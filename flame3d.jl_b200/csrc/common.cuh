@@ -160,50 +160,49 @@ __device__ __forceinline__ T minmod(T a, T b) {  // schemes.jl:26-28
     return (a * b > 0) ? ((fabs(a) > fabs(b)) ? b : a) : T(0);
 }
 
+// WENO-Z weights and combination, schemes.jl:152-162: the smoothness indicators come in the
+// arithmetic type T, the weights are formed in FP64 (in FP32, q = τ/(1e-26 + β) overflows when
+// a one-sided split makes β exactly 0, and ∞·0 would poison the flux).
+template <typename T>
+__device__ __forceinline__ T wenoz_combine(T s11_, T s22_, T s33_, T v1, T v2, T v3) {
+    const double s11 = s11_, s22 = s22_, s33 = s33_;
+    const double tau = fabs(s11 - s33);
+    double q, a1, a2, a3;
+    q = tau / (kWenoEps + s11), a1 = (1 + q * q) * 1;
+    q = tau / (kWenoEps + s22), a2 = (1 + q * q) * 6;
+    q = tau / (kWenoEps + s33), a3 = (1 + q * q) * 3;
+    const double invsum = 1 / (a1 + a2 + a3);
+    return T((1.0 / 6.0) * invsum * (a1 * double(v1) + a2 * double(v2) + a3 * double(v3)));
+}
+
 // WENO-Z5 positive-flux reconstruction from V1..V5 = F+[c-3..c+1], schemes.jl:139-162
 template <typename T>
 __device__ __forceinline__ T wenoz_plus(T V1, T V2, T V3, T V4, T V5) {
-    const T tmp1 = T(13.0 / 12.0), tmp2 = T(1.0 / 6.0), q4 = T(0.25), eps = T(kWenoEps);
+    const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);
     T a, b;
     a = V1 - 2 * V2 + V3, b = V1 - 4 * V2 + 3 * V3;
-    T s11 = tmp1 * (a * a) + q4 * (b * b);
+    const T s11 = tmp1 * (a * a) + q4 * (b * b);
     a = V2 - 2 * V3 + V4, b = V2 - V4;
-    T s22 = tmp1 * (a * a) + q4 * (b * b);
+    const T s22 = tmp1 * (a * a) + q4 * (b * b);
     a = V3 - 2 * V4 + V5, b = 3 * V3 - 4 * V4 + V5;
-    T s33 = tmp1 * (a * a) + q4 * (b * b);
-    T tau = fabs(s11 - s33);
-    T q;
-    q = tau / (eps + s11), s11 = (1 + q * q) * 1;
-    q = tau / (eps + s22), s22 = (1 + q * q) * 6;
-    q = tau / (eps + s33), s33 = (1 + q * q) * 3;
-    T invsum = 1 / (s11 + s22 + s33);
-    T v1 = 2 * V1 - 7 * V2 + 11 * V3;
-    T v2 = -V2 + 5 * V3 + 2 * V4;
-    T v3 = 2 * V3 + 5 * V4 - V5;
-    return tmp2 * invsum * (s11 * v1 + s22 * v2 + s33 * v3);
+    const T s33 = tmp1 * (a * a) + q4 * (b * b);
+    return wenoz_combine<T>(s11, s22, s33, 2 * V1 - 7 * V2 + 11 * V3, -V2 + 5 * V3 + 2 * V4,
+                            2 * V3 + 5 * V4 - V5);
 }
 
 // WENO-Z5 negative-flux reconstruction from V1..V5 = F-[c-2..c+2], schemes.jl:164-187
 template <typename T>
 __device__ __forceinline__ T wenoz_minus(T V1, T V2, T V3, T V4, T V5) {
-    const T tmp1 = T(13.0 / 12.0), tmp2 = T(1.0 / 6.0), q4 = T(0.25), eps = T(kWenoEps);
+    const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);
     T a, b;
     a = V5 - 2 * V4 + V3, b = V5 - 4 * V4 + 3 * V3;
-    T s11 = tmp1 * (a * a) + q4 * (b * b);
+    const T s11 = tmp1 * (a * a) + q4 * (b * b);
     a = V2 - 2 * V3 + V4, b = V4 - V2;
-    T s22 = tmp1 * (a * a) + q4 * (b * b);
+    const T s22 = tmp1 * (a * a) + q4 * (b * b);
     a = V3 - 2 * V2 + V1, b = 3 * V3 - 4 * V2 + V1;
-    T s33 = tmp1 * (a * a) + q4 * (b * b);
-    T tau = fabs(s11 - s33);
-    T q;
-    q = tau / (eps + s11), s11 = (1 + q * q) * 1;
-    q = tau / (eps + s22), s22 = (1 + q * q) * 6;
-    q = tau / (eps + s33), s33 = (1 + q * q) * 3;
-    T invsum = 1 / (s11 + s22 + s33);
-    T v1 = 11 * V3 - 7 * V4 + 2 * V5;
-    T v2 = -V4 + 5 * V3 + 2 * V2;
-    T v3 = 2 * V3 + 5 * V2 - V1;
-    return tmp2 * invsum * (s11 * v1 + s22 * v2 + s33 * v3);
+    const T s33 = tmp1 * (a * a) + q4 * (b * b);
+    return wenoz_combine<T>(s11, s22, s33, 11 * V3 - 7 * V4 + 2 * V5, -V4 + 5 * V3 + 2 * V2,
+                            2 * V3 + 5 * V2 - V1);
 }
 
 // One face of the hybrid scheme, schemes.jl:110-199.  p[0..6] = F+[c-3..c+3] (F+[c-4] has

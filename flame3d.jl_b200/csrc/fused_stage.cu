@@ -1,99 +1,124 @@
 // fused_stage.cu — one launch per SSP-RK3 stage on periodic grids (sm_100a).
 //
-// A CTA owns a 16 x 8 x 8 tile of interior cells and performs, for that tile, everything
+// A CTA owns a TX x TY x TZ tile of interior cells and performs, for that tile, everything
 // solver.jl:298-326 does in ~30 launches:
-//   point phase   shock sensor (schemes.jl:1-24), transport law (stand-in for thermo.jl:371),
-//                 1/max(ρ, eps) for the mass fractions, into shared memory;
+//   point phase   shock sensor (schemes.jl:1-24) and 1/max(ρ, eps) (the mass-fraction factor of
+//                 thermo.jl:391) on the tile and its halo, into shared memory;
 //   sweeps        per direction, in chunks: Steger-Warming split of every pencil point into
 //                 shared memory (split.jl:17-130), hybrid UP7 / WENO-Z / minmod face fluxes
 //                 (schemes.jl:86-437), viscous and species-diffusion face fluxes
 //                 (viscous.jl:1-665) and the face differences into per-cell accumulators;
 //   epilogue      div (div.jl), RK3 combination (utils.jl:95-112), c2Prim with the Newton
-//                 temperature solve (utils.jl:2-48, thermo.jl:231-282), and the writes of the
+//                 temperature solve (utils.jl:2-48, thermo.jl:231-282), the transport law of
+//                 the new state (the stand-in for thermo.jl:371-403), and the writes of the
 //                 result and of its periodic ghost images.
-// Split fluxes are computed once per point and direction (plus the pencil halo); face
-// fluxes are computed once per face.  The only HBM traffic is the stage's inputs (with halo
-// re-reads served by L2) and its outputs.
+// Split fluxes are computed once per point and direction (plus the pencil halo); face fluxes
+// once per face; μ, λ, D once per cell (by the epilogue of the stage before).  HBM traffic is
+// the stage's inputs (halo re-reads are served by L2) and its outputs.
 //
-// Template parameters: NS species (compile-time loops), QT storage type of the primitive
-// array Q, CT arithmetic type of split / reconstruction / viscous fluxes.  The plain path is
-// <NS, double, double>; the mixed path is <NS, float, float> with U, Un, rhoi, metrics, the
-// accumulators and the Newton solve kept in FP64.
+// Template parameters: a tile configuration, NS species (compile-time loops), QT the storage
+// type of the primitive and transport arrays, CT the arithmetic type of split, reconstruction
+// and viscous fluxes.  The plain path is <cfg, NS, double, double>; the mixed path is
+// <cfg, NS, float, float> with U, Un, rho_i, metrics, accumulators, the WENO-Z weights and the
+// Newton solve kept in FP64.
+//
+// All indices are 32-bit: the host checks that every array holds fewer than 2^31 elements.
 
 #include "common.cuh"
+
+int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
+                       const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *th,
+                       const FlameTransport *tr, int precision, void *scratch);
 
 namespace flame {
 namespace fused {
 
-constexpr int TX = 16, TY = 8, TZ = 8, NT = 256;
-constexpr int CPT = TX * TY * TZ / NT;  // cells per thread (4): z = cz0 + 2*m
-constexpr int BX1 = TX + 2, BY1 = TY + 2, BZ1 = TZ + 2, NB1 = BX1 * BY1 * BZ1;  // box [-1,T]
-constexpr int BX2 = TX + 4, BY2 = TY + 4, BZ2 = TZ + 4, NB2 = BX2 * BY2 * BZ2;  // box [-2,T+1]
+// Tile configurations the autotuner chooses from.  ZC / YC are the chunk depths of the x/y and
+// z sweeps so that a chunk holds exactly NT cells: one owned cell per thread and chunk in the
+// x/y sweeps; all owned cells of the threads with cy / YC == chunk in the z sweep.
+template <int TX_, int TY_, int TZ_, int NT_, int MINB_>
+struct TileCfg {
+    static constexpr int TX = TX_, TY = TY_, TZ = TZ_, NT = NT_, MINB = MINB_;
+    static constexpr int CELLS = TX * TY * TZ;
+    static constexpr int CPT = CELLS / NT;
+    static constexpr int ZC = NT / (TX * TY);
+    static constexpr int YC = NT / (TX * TZ);
+    static_assert(CELLS % NT == 0 && NT % (TX * TY) == 0 && NT % (TX * TZ) == 0, "tile");
+    static_assert(TZ % ZC == 0 && TY % YC == 0 && CPT == TZ / ZC, "chunks");
+    static constexpr int BX1 = TX + 2, BY1 = TY + 2, BZ1 = TZ + 2, NB1 = BX1 * BY1 * BZ1;
+    static constexpr int BX2 = TX + 4, BY2 = TY + 4, BZ2 = TZ + 4, NB2 = BX2 * BY2 * BZ2;
+};
 
-template <int NS>
-struct Cfg {
-    static constexpr int ZC = NS <= 4 ? 2 : 1;  // planes per chunk (x, y sweeps)
-    static constexpr int YC = ZC;               // rows per chunk (z sweep)
-    static constexpr int VF = 10 + 2 * NS;      // split values per point
-    static constexpr int VG = 5 + NS;           // face values
-    static constexpr int NPX = (TX + 6) * TY * ZC, NPY = TX * (TY + 6) * ZC,
-                         NPZ = TX * YC * (TZ + 6);
-    static constexpr int NFX = (TX + 1) * TY * ZC, NFY = TX * (TY + 1) * ZC,
-                         NFZ = TX * YC * (TZ + 1);
+using Cfg16x8x8 = TileCfg<16, 8, 8, 256, 1>;
+using Cfg16x8x8b2 = TileCfg<16, 8, 8, 256, 2>;
+using Cfg8x8x8 = TileCfg<8, 8, 8, 256, 2>;
+
+template <class T, int NS>
+struct Layout {
+    static constexpr int VF = 10 + 2 * NS;  // split values per point
+    static constexpr int VG = 5 + NS;       // face values
+    static constexpr int NPX = (T::TX + 6) * T::TY * T::ZC, NPY = T::TX * (T::TY + 6) * T::ZC,
+                         NPZ = T::TX * T::YC * (T::TZ + 6);
+    static constexpr int NFX = (T::TX + 1) * T::TY * T::ZC, NFY = T::TX * (T::TY + 1) * T::ZC,
+                         NFZ = T::TX * T::YC * (T::TZ + 1);
     static constexpr int NPMAX = NPX > NPY ? (NPX > NPZ ? NPX : NPZ) : (NPY > NPZ ? NPY : NPZ);
     static constexpr int NFMAX = NFX > NFY ? (NFX > NFZ ? NFX : NFZ) : (NFY > NFZ ? NFY : NFZ);
 };
 
 template <typename QT>
 struct Args {
-    Dims D;
+    int nx, ny, nz, ng, tx, ty, tz, np, sy, sz;
     int stage;
-    double dt, ca, cb;  // RK3 combination U = ca*U + cb*Un (stage 2, 3)
+    double dt, ca, cb;  // RK3 combination U = ca*U + cb*Un (stages 2, 3)
     double *U, *Un;
     const QT *Qi;
     QT *Qo;
+    const QT *Ti;  // μ, λ, D of the stage input
+    QT *To;        // μ, λ, D of the stage result
     const double *ri;
     double *ro, *rn;
-    FlameMetrics m;
+    const double *met[10];  // ξx ξy ξz ηx ηy ηz ζx ζy ζz J
     FlameThermo th;
     FlameTransport tr;
 };
 
-template <int NS, typename CT>
+template <class T, int NS, typename CT>
 constexpr size_t smem_bytes() {
+    using L = Layout<T, NS>;
     // working arrays, or the epilogue's accumulator hand-off if that is larger
-    constexpr size_t work = sizeof(CT) * (4 * NB1 + NB2 + Cfg<NS>::VF * Cfg<NS>::NPMAX +
-                                          Cfg<NS>::VG * Cfg<NS>::NFMAX);
-    constexpr size_t acc = sizeof(double) * CPT * Cfg<NS>::VG * NT;
+    constexpr size_t work =
+        sizeof(CT) * (T::NB1 + T::NB2 + L::VF * L::NPMAX + L::VG * L::NFMAX);
+    constexpr size_t acc = sizeof(double) * T::CPT * L::VG * T::NT;
     return work > acc ? work : acc;
 }
 
-__device__ __forceinline__ long long clampll(long long v, long long lo, long long hi) {
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
     return v < lo ? lo : (v > hi ? hi : v);
 }
 
-template <typename CT>
-__device__ __forceinline__ CT ld(const double *p, long long i) {
-    return CT(__ldg(p + i));
-}
-template <typename CT>
-__device__ __forceinline__ CT ld(const float *p, long long i) {
+template <typename CT, typename T>
+__device__ __forceinline__ CT ldg(const T *p, int i) {
     return CT(__ldg(p + i));
 }
 
-// Steger-Warming splitting of the Euler flux along metric (A1, A2, A3), split.jl:17-89.
+// Steger-Warming splitting of the Euler flux along metric (A1, A2, A3), split.jl:17-89, with
+// the reference's divisions folded into two reciprocals and one reciprocal square root (the
+// results differ from the reference's rounding by a few ulp, far inside the 1e-12 bound).
 template <typename CT>
 __device__ __forceinline__ void sw_split(CT rho, CT u, CT v, CT w, CT p, CT ei, CT A1, CT A2,
                                          CT A3, CT *fp, CT *fm) {
-    const CT gam = p / ei + 1;
-    const CT cs = sqrt(gam * p / rho);
-    CT ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
+    const CT h = CT(0.5);
+    const CT gam = p * (CT(1) / ei) + 1;
+    const CT gm1 = gam - 1;
+    const CT inv = CT(1) / (rho * gam * gm1);  // 1/(ρ γ (γ-1))
+    const CT cs = sqrt(gam * p * (gam * gm1 * inv));
+    const CT r2 = A1 * A1 + A2 * A2 + A3 * A3;
+    const CT rs = rsqrt(r2);
+    const CT ss = r2 * rs;
     const CT E1 = A1 * u + A2 * v + A3 * w;
     const CT E2 = E1 - cs * ss;
     const CT E3 = E1 + cs * ss;
-    ss = 1 / ss;
-    A1 *= ss, A2 *= ss, A3 *= ss;
-    const CT h = CT(0.5);
+    A1 *= rs, A2 *= rs, A3 *= rs;
     const CT E1P = (E1 + fabs(E1)) * h, E2P = (E2 + fabs(E2)) * h, E3P = (E3 + fabs(E3)) * h;
     const CT E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
     const CT uc1 = u - cs * A1, uc2 = u + cs * A1;
@@ -101,10 +126,10 @@ __device__ __forceinline__ void sw_split(CT rho, CT u, CT v, CT w, CT p, CT ei, 
     const CT wc1 = w - cs * A3, wc2 = w + cs * A3;
     const CT vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * h;
     const CT vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * h;
-    const CT vv = (gam - 1) * (u * u + v * v + w * w);
-    const CT W2 = (3 - gam) / (2 * (gam - 1)) * (cs * cs);
-    const CT tmp1 = rho / (2 * gam);
-    const CT tmp2 = 2 * (gam - 1);
+    const CT vv = gm1 * (u * u + v * v + w * w);
+    const CT W2 = (3 - gam) * (h * rho * gam * inv) * (cs * cs);  // (3-γ)/(2(γ-1)) c²
+    const CT tmp1 = h * rho * (rho * gm1 * inv);                  // ρ/(2γ)
+    const CT tmp2 = 2 * gm1;
     fp[0] = tmp1 * (tmp2 * E1P + E2P + E3P);
     fp[1] = tmp1 * (tmp2 * E1P * u + E2P * uc1 + E3P * uc2);
     fp[2] = tmp1 * (tmp2 * E1P * v + E2P * vc1 + E3P * vc2);
@@ -117,136 +142,103 @@ __device__ __forceinline__ void sw_split(CT rho, CT u, CT v, CT w, CT p, CT ei, 
     fm[4] = tmp1 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
 }
 
-// Geometry of a sweep chunk along direction DIR.  "a" runs along the sweep, (b1, b2) across.
-template <int NS, int DIR>
-struct Sweep {
-    using C = Cfg<NS>;
-    static constexpr int L = DIR == 0 ? TX : (DIR == 1 ? TY : TZ);        // cells along
-    static constexpr int C1 = DIR == 0 ? TY : TX;                         // first cross extent
-    static constexpr int C2 = DIR == 2 ? C::YC : C::ZC;                   // chunk depth
-    static constexpr int NCH = DIR == 2 ? TY / C::YC : TZ / C::ZC;        // chunks
-    static constexpr int NP = (L + 6) * C1 * C2;
-    static constexpr int NF = (L + 1) * C1 * C2;
-    // tile-relative cell of (along a, cross b1, chunk-local b2) in chunk ch
-    __device__ static void cell(int a, int b1, int b2, int ch, int &x, int &y, int &z) {
-        if (DIR == 0) x = a, y = b1, z = ch * C2 + b2;
-        else if (DIR == 1) x = b1, y = a, z = ch * C2 + b2;
-        else x = b1, y = ch * C2 + b2, z = a;
+// Transport law of one point (stand-in for mixtureProperties, thermo.jl:289-369); writes μ, λ, D.
+template <int NS>
+__device__ __forceinline__ void transport_point(const FlameThermo &th, const FlameTransport &tr,
+                                                double T, double rho_raw, const double *r,
+                                                double &mu, double &lam, double &D) {
+    if (tr.law == 0) {
+        mu = tr.mu_ref, lam = tr.lambda_ref, D = tr.D_ref;
+        return;
     }
-};
+    const double rho = jmax(rho_raw, kEps);
+    const double rinv = 1 / rho;
+    const double T2 = T * T, T3 = T2 * T, T4 = T2 * T2;
+    double cpm = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n)
+        cpm += cp_spec(th, n, T, T2, T3, T4) * jmax(r[n] * rinv, 0.0) / th.mw[n];
+    cpm *= th.Ru;
+    mu = tr.mu_ref * pow(T / tr.T_ref, tr.exponent);
+    lam = cpm * mu / tr.Pr;
+    D = lam / (rho * cpm);
+}
 
-template <int NS, typename QT, typename CT>
+template <class T, int NS, typename QT, typename CT>
 struct Tile {
-    using C = Cfg<NS>;
+    using L = Layout<T, NS>;
+    static constexpr int TX = T::TX, TY = T::TY, TZ = T::TZ, NT = T::NT, CPT = T::CPT;
     const Args<QT> &A;
-    const long long X0, Y0, Z0;  // interior index of the tile's first cell
-    const long long sy, sz, np;
-    CT *sPhi, *sMu, *sLam, *sD, *sRinv, *sF, *sG;
+    const int X0, Y0, Z0;  // interior index of the tile's first cell
+    CT *sPhi, *sRinv, *sF, *sG;
 
     __device__ Tile(const Args<QT> &a, CT *smem)
-        : A(a),
-          X0((long long)blockIdx.x * TX),
-          Y0((long long)blockIdx.y * TY),
-          Z0((long long)blockIdx.z * TZ),
-          sy(a.D.tx),
-          sz(a.D.tx * a.D.ty),
-          np(a.D.np) {
+        : A(a), X0(blockIdx.x * TX), Y0(blockIdx.y * TY), Z0(blockIdx.z * TZ) {
         sPhi = smem;
-        sMu = sPhi + NB1;
-        sLam = sMu + NB1;
-        sD = sLam + NB1;
-        sRinv = sD + NB1;
-        sF = sRinv + NB2;
-        sG = sF + C::VF * C::NPMAX;
+        sRinv = sPhi + T::NB1;
+        sF = sRinv + T::NB2;
+        sG = sF + L::VF * L::NPMAX;
     }
 
     // ghosted linear index of tile-relative cell (x, y, z), clamped into the array
-    __device__ long long gidx(int x, int y, int z) const {
-        const long long gx = clampll(X0 + A.D.ng + x, 0, A.D.tx - 1);
-        const long long gy = clampll(Y0 + A.D.ng + y, 0, A.D.ty - 1);
-        const long long gz = clampll(Z0 + A.D.ng + z, 0, A.D.tz - 1);
-        return gx + sy * (gy + A.D.ty * gz);
+    __device__ int gidx(int x, int y, int z) const {
+        const int gx = clampi(X0 + A.ng + x, 0, A.tx - 1);
+        const int gy = clampi(Y0 + A.ng + y, 0, A.ty - 1);
+        const int gz = clampi(Z0 + A.ng + z, 0, A.tz - 1);
+        return gx + A.sy * gy + A.sz * gz;
     }
     // ghosted index of the right cell of a DIR face, clamped so that the whole viscous stencil
     // (normal -2..+1, tangential ±2) stays inside the array even for tiles past the domain end
     template <int DIR>
-    __device__ long long gidx_face(int x, int y, int z) const {
-        const int ng = A.D.ng;
-        const long long gx = clampll(X0 + ng + x, ng, A.D.nx + ng - (DIR != 0));
-        const long long gy = clampll(Y0 + ng + y, ng, A.D.ny + ng - (DIR != 1));
-        const long long gz = clampll(Z0 + ng + z, ng, A.D.nz + ng - (DIR != 2));
-        return gx + sy * (gy + A.D.ty * gz);
+    __device__ int gidx_face(int x, int y, int z) const {
+        const int ng = A.ng;
+        const int gx = clampi(X0 + ng + x, ng, A.nx + ng - (DIR != 0));
+        const int gy = clampi(Y0 + ng + y, ng, A.ny + ng - (DIR != 1));
+        const int gz = clampi(Z0 + ng + z, ng, A.nz + ng - (DIR != 2));
+        return gx + A.sy * gy + A.sz * gz;
     }
     __device__ static int b1i(int x, int y, int z) {
-        return (x + 1) + BX1 * ((y + 1) + BY1 * (z + 1));
+        return (x + 1) + T::BX1 * ((y + 1) + T::BY1 * (z + 1));
     }
     __device__ static int b2i(int x, int y, int z) {
-        return (x + 2) + BX2 * ((y + 2) + BY2 * (z + 2));
+        return (x + 2) + T::BX2 * ((y + 2) + T::BY2 * (z + 2));
     }
 
     // ---------------------------------------------------------------- point phase
     __device__ void point_phase() {
         const QT *Q = A.Qi;
-        // 1/max(ρ, eps) on the box [-2, T+1]^3 (mixture: thermo.jl:391)
-        for (int p = threadIdx.x; p < NB2; p += NT) {
-            const int x = p % BX2 - 2, y = (p / BX2) % BY2 - 2, z = p / (BX2 * BY2) - 2;
-            const long long g = gidx(x, y, z);
-            sRinv[p] = CT(1) / CT(jmax(double(Q[g]), kEps));
+        for (int p = threadIdx.x; p < T::NB2; p += NT) {
+            const int x = p % T::BX2 - 2, y = (p / T::BX2) % T::BY2 - 2, z = p / (T::BX2 * T::BY2) - 2;
+            sRinv[p] = CT(1) / CT(jmax(double(Q[gidx(x, y, z)]), kEps));
         }
-        // sensor, μ, λ, D on the box [-1, T]^3
-        for (int p = threadIdx.x; p < NB1; p += NT) {
-            const int x = p % BX1 - 1, y = (p / BX1) % BY1 - 1, z = p / (BX1 * BY1) - 1;
-            long long g = gidx(x, y, z);
-            // schemes.jl:10-22; the neighbours of a clamped point stay inside the array
-            {
-                const long long gx = g % sy, gy = (g / sy) % A.D.ty, gz = g / sz;
-                const long long gc = clampll(gx, 1, A.D.tx - 2) +
-                                     sy * (clampll(gy, 1, A.D.ty - 2) +
-                                           A.D.ty * clampll(gz, 1, A.D.tz - 2));
-                const QT *P = Q + 4 * np;
-                const CT P2 = CT(P[gc]);
-                CT a1 = CT(P[gc - 1]), a3 = CT(P[gc + 1]);
-                const CT phx = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
-                a1 = CT(P[gc - sy]), a3 = CT(P[gc + sy]);
-                const CT phy = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
-                a1 = CT(P[gc - sz]), a3 = CT(P[gc + sz]);
-                const CT phz = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
-                sPhi[p] = phx + phy + phz;
-            }
-            // transport law in place of mixtureProperties (thermo.jl:289-369)
-            CT mu, lam, dd;
-            if (A.tr.law == 0) {
-                mu = CT(A.tr.mu_ref), lam = CT(A.tr.lambda_ref), dd = CT(A.tr.D_ref);
-            } else {
-                const double T = double(Q[g + 5 * np]);
-                const double rho = jmax(double(Q[g]), kEps);
-                const double rinv = 1 / rho;
-                const double T2 = T * T, T3 = T2 * T, T4 = T2 * T2;
-                double cpm = 0;
-#pragma unroll
-                for (int n = 0; n < NS; ++n) {
-                    const double Y = jmax(A.ri[g + n * np] * rinv, 0.0);
-                    cpm += cp_spec(A.th, n, T, T2, T3, T4) * Y / A.th.mw[n];
-                }
-                cpm *= A.th.Ru;
-                const double m = A.tr.mu_ref * pow(T / A.tr.T_ref, A.tr.exponent);
-                const double l = cpm * m / A.tr.Pr;
-                mu = CT(m), lam = CT(l), dd = CT(l / (rho * cpm));
-            }
-            sMu[p] = mu, sLam[p] = lam, sD[p] = dd;
+        const QT *P = Q + 4 * A.np;
+        for (int p = threadIdx.x; p < T::NB1; p += NT) {
+            const int x = p % T::BX1 - 1, y = (p / T::BX1) % T::BY1 - 1, z = p / (T::BX1 * T::BY1) - 1;
+            // schemes.jl:10-22 with the exact divisions: the branch thresholds see the same ϕ
+            const int gx = clampi(X0 + A.ng + x, 1, A.tx - 2);
+            const int gy = clampi(Y0 + A.ng + y, 1, A.ty - 2);
+            const int gz = clampi(Z0 + A.ng + z, 1, A.tz - 2);
+            const int gc = gx + A.sy * gy + A.sz * gz;
+            const CT P2 = CT(P[gc]);
+            CT a1 = CT(P[gc - 1]), a3 = CT(P[gc + 1]);
+            const CT phx = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+            a1 = CT(P[gc - A.sy]), a3 = CT(P[gc + A.sy]);
+            const CT phy = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+            a1 = CT(P[gc - A.sz]), a3 = CT(P[gc + A.sz]);
+            const CT phz = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+            sPhi[p] = phx + phy + phz;
         }
     }
 
     // ---------------------------------------------------------------- split of one point
     template <int DIR>
-    __device__ void split_point(long long g, CT *out, int stride) const {
-        const double *Ax = DIR == 0 ? A.m.dxidx : (DIR == 1 ? A.m.detadx : A.m.dzetadx);
-        const double *Ay = DIR == 0 ? A.m.dxidy : (DIR == 1 ? A.m.detady : A.m.dzetady);
-        const double *Az = DIR == 0 ? A.m.dxidz : (DIR == 1 ? A.m.detadz : A.m.dzetadz);
+    __device__ void split_point(int g, CT *out, int stride) const {
+        const double *Ax = A.met[3 * DIR], *Ay = A.met[3 * DIR + 1], *Az = A.met[3 * DIR + 2];
         const QT *Q = A.Qi;
-        const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]),
-                 p = CT(Q[g + 4 * np]), ei = CT(Q[g + 6 * np]);
-        const CT A1 = ld<CT>(Ax, g), A2 = ld<CT>(Ay, g), A3 = ld<CT>(Az, g);
+        const int np = A.np;
+        const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]),
+                 w = CT(Q[g + 3 * np]), p = CT(Q[g + 4 * np]), ei = CT(Q[g + 6 * np]);
+        const CT A1 = ldg<CT>(Ax, g), A2 = ldg<CT>(Ay, g), A3 = ldg<CT>(Az, g);
         CT fp[5], fm[5];
         sw_split<CT>(rho, u, v, w, p, ei, A1, A2, A3, fp, fm);
 #pragma unroll
@@ -265,41 +257,39 @@ struct Tile {
 
     // ---------------------------------------------------------------- viscous face
     // Face between tile cells (x,y,z) - e_DIR and (x,y,z); ghosted index g of the right cell.
-    // Writes G[1..4] -= Fv (viscous.jl:1-428) and G[5+n] -= Fd_n (viscous.jl:430-665), so that
-    // G holds F_inviscid - F_viscous with the sign convention of div.jl.
+    // Subtracts Fv (viscous.jl:1-428) from G[1..4] and Fd_n (viscous.jl:430-665) from G[5+n],
+    // so G holds F_inviscid - F_viscous with the sign convention of div.jl.
     template <int DIR>
-    __device__ void viscous_face(long long g, int x, int y, int z, CT *G) const {
+    __device__ void viscous_face(int g, int x, int y, int z, CT *G) const {
         constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
-        const long long sn = DIR == 0 ? 1 : (DIR == 1 ? sy : sz);
-        const long long s1 = D1 == 0 ? 1 : (D1 == 1 ? sy : sz);
-        const long long s2 = D2 == 0 ? 1 : (D2 == 1 ? sy : sz);
-        const int xl = x - (DIR == 0), yl = y - (DIR == 1), zl = z - (DIR == 2);
-        const int bR = b1i(x, y, z), bL = b1i(xl, yl, zl);
+        const int np = A.np;
+        const int sn = DIR == 0 ? 1 : (DIR == 1 ? A.sy : A.sz);
+        const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
+        const int s2 = D2 == 0 ? 1 : (D2 == 1 ? A.sy : A.sz);
         const QT *Q = A.Qi;
-        const double *M[9] = {A.m.dxidx,   A.m.dxidy,   A.m.dxidz,   A.m.detadx, A.m.detady,
-                              A.m.detadz,  A.m.dzetadx, A.m.dzetady, A.m.dzetadz};
         const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
         CT met[9];
 #pragma unroll
-        for (int a = 0; a < 9; ++a) met[a] = (ld<CT>(M[a], g - sn) + ld<CT>(M[a], g)) * h;
-        const CT Jac = (ld<CT>(A.m.J, g - sn) + ld<CT>(A.m.J, g)) * h;
-        const CT mui = (sMu[bL] + sMu[bR]) * h;
-        const CT lami = (sLam[bL] + sLam[bR]) * h;
+        for (int a = 0; a < 9; ++a) met[a] = (ldg<CT>(A.met[a], g - sn) + ldg<CT>(A.met[a], g)) * h;
+        const CT Jac = (ldg<CT>(A.met[9], g - sn) + ldg<CT>(A.met[9], g)) * h;
+        const QT *Tr = A.Ti;
+        const CT mui = (ldg<CT>(Tr, g - sn) + ldg<CT>(Tr, g)) * h;
+        const CT lami = (ldg<CT>(Tr + np, g - sn) + ldg<CT>(Tr + np, g)) * h;
+        const CT DL = ldg<CT>(Tr + 2 * np, g - sn), DR = ldg<CT>(Tr + 2 * np, g);
 
         // species diffusion first: it produces Fh for the energy flux (viscous.jl:446-505)
         const CT rho = (CT(Q[g - sn]) + CT(Q[g])) * h;
-        const CT T = (CT(Q[g - sn + 5 * np]) + CT(Q[g + 5 * np])) * h;
+        const CT Tf = (CT(Q[g - sn + 5 * np]) + CT(Q[g + 5 * np])) * h;
         const int b2R = b2i(x, y, z);
-        const int o_n = DIR == 0 ? 1 : (DIR == 1 ? BX2 : BX2 * BY2);
-        const int o_1 = D1 == 0 ? 1 : (D1 == 1 ? BX2 : BX2 * BY2);
-        const int o_2 = D2 == 0 ? 1 : (D2 == 1 ? BX2 : BX2 * BY2);
+        constexpr int o_n = DIR == 0 ? 1 : (DIR == 1 ? T::BX2 : T::BX2 * T::BY2);
+        constexpr int o_1 = D1 == 0 ? 1 : (D1 == 1 ? T::BX2 : T::BX2 * T::BY2);
+        constexpr int o_2 = D2 == 0 ? 1 : (D2 == 1 ? T::BX2 : T::BX2 * T::BY2);
         CT Vk1[NS], Vk2[NS], Vk3[NS], Yf[NS];
         CT sum1 = 0, sum2 = 0, sum3 = 0;
-        const CT DL = sD[bL], DR = sD[bR];
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
             const double *r = A.ri + n * np;
-            // Y = max(ρi / max(ρ, eps), 0) at the stencil points
+            // Y = max(ρi / max(ρ, eps), 0) at the stencil points (mixture, thermo.jl:391-394)
 #define YAT(off, boff) (fmax(CT(r[g + (off)]) * sRinv[b2R + (boff)], CT(0)))
             const CT y0 = YAT(0, 0), ym = YAT(-sn, -o_n);
             const CT yp = YAT(sn, o_n), ymm = YAT(-2 * sn, -2 * o_n);
@@ -322,7 +312,7 @@ struct Tile {
         const CT *md = met + 3 * DIR;
         CT fh1 = 0, fh2 = 0, fh3 = 0;
         {
-            const double Td = double(T);
+            const double Td = double(Tf);
             const double T2 = 0.5 * Td * Td, T3 = 2.0 / 3.0 * T2 * Td, T4 = T2 * T2,
                          T5 = 0.8 * T4 * Td;
 #pragma unroll
@@ -372,33 +362,43 @@ struct Tile {
         G[4] -= md[0] * E1 + md[1] * E2 + md[2] * E3;
     }
 
+    // tile-relative cell of (along a, cross b1, chunk-local b2) in chunk ch of sweep DIR
+    template <int DIR>
+    __device__ static void sweep_cell(int a, int b, int ch, int &x, int &y, int &z) {
+        if (DIR == 0) x = a, y = b % TY, z = ch * T::ZC + b / TY;
+        else if (DIR == 1) y = a, x = b % TX, z = ch * T::ZC + b / TX;
+        else z = a, x = b % TX, y = ch * T::YC + b / TX;
+    }
+
     // ---------------------------------------------------------------- one sweep direction
     template <int DIR>
-    __device__ void sweep(double (&acc)[CPT][C::VG]) {
-        using SW = Sweep<NS, DIR>;
+    __device__ void sweep(double (&acc)[CPT][L::VG]) {
+        constexpr int LEN = DIR == 0 ? TX : (DIR == 1 ? TY : TZ);
+        constexpr int NP = DIR == 0 ? L::NPX : (DIR == 1 ? L::NPY : L::NPZ);
+        constexpr int NF = DIR == 0 ? L::NFX : (DIR == 1 ? L::NFY : L::NFZ);
+        constexpr int NCH = DIR == 2 ? TY / T::YC : TZ / T::ZC;
         const int tid = threadIdx.x;
         const int cx = tid % TX, cy = (tid / TX) % TY, cz0 = tid / (TX * TY);
 #pragma unroll 1
-        for (int ch = 0; ch < SW::NCH; ++ch) {
+        for (int ch = 0; ch < NCH; ++ch) {
             // split fluxes of every pencil point of the chunk
-            for (int p = tid; p < SW::NP; p += NT) {
-                const int a = p % (SW::L + 6) - 3, b = p / (SW::L + 6);
+            for (int p = tid; p < NP; p += NT) {
                 int x, y, z;
-                SW::cell(a, b % SW::C1, b / SW::C1, ch, x, y, z);
-                split_point<DIR>(gidx(x, y, z), sF + p, C::NPMAX);
+                sweep_cell<DIR>(p % (LEN + 6) - 3, p / (LEN + 6), ch, x, y, z);
+                split_point<DIR>(gidx(x, y, z), sF + p, L::NPMAX);
             }
             __syncthreads();
             // face fluxes
-            for (int f = tid; f < SW::NF; f += NT) {
-                const int a = f % (SW::L + 1), b = f / (SW::L + 1);
+            for (int f = tid; f < NF; f += NT) {
+                const int a = f % (LEN + 1), b = f / (LEN + 1);
                 int x, y, z;
-                SW::cell(a, b % SW::C1, b / SW::C1, ch, x, y, z);
+                sweep_cell<DIR>(a, b, ch, x, y, z);
                 const int xl = x - (DIR == 0), yl = y - (DIR == 1), zl = z - (DIR == 2);
                 const CT phif = CT(jmax(double(sPhi[b1i(xl, yl, zl)]), double(sPhi[b1i(x, y, z)])));
-                const int p0 = a + (SW::L + 6) * b;  // point index of along-coordinate a-3
-                CT G[C::VG];
+                const int p0 = a + (LEN + 6) * b;  // point index of along-coordinate a-3
+                CT G[L::VG];
 #pragma unroll
-                for (int n = 0; n < C::VG; ++n) {
+                for (int n = 0; n < L::VG; ++n) {
                     const int vp = n < 5 ? n : 5 + n;  // F+ row (species rows start at 10)
                     const int vm = n < 5 ? 5 + n : 5 + NS + n;
                     // the hybrid face reads F±[c-3..c+2] only (UP7[1] = 0 drops F+[c-4], and
@@ -406,36 +406,36 @@ struct Tile {
                     CT pv[7], mv[7];
 #pragma unroll
                     for (int i = 0; i < 6; ++i) {
-                        pv[i] = sF[vp * C::NPMAX + p0 + i];
-                        mv[i] = sF[vm * C::NPMAX + p0 + i];
+                        pv[i] = sF[vp * L::NPMAX + p0 + i];
+                        mv[i] = sF[vm * L::NPMAX + p0 + i];
                     }
                     pv[6] = mv[6] = CT(0);
                     G[n] = hybrid_face7<CT>(pv, mv, phif);
                 }
                 viscous_face<DIR>(gidx_face<DIR>(x, y, z), x, y, z, G);
 #pragma unroll
-                for (int n = 0; n < C::VG; ++n) sG[n * C::NFMAX + f] = G[n];
+                for (int n = 0; n < L::VG; ++n) sG[n * L::NFMAX + f] = G[n];
             }
             __syncthreads();
             // face differences into the owned cells of this chunk
 #pragma unroll
             for (int m = 0; m < CPT; ++m) {
-                const int z = cz0 + 2 * m;
+                const int z = cz0 + T::ZC * m;
                 bool in;
                 int a, b;
                 if (DIR == 2) {
-                    in = (cy / C::YC) == ch;
-                    a = z, b = cx + TX * (cy - ch * C::YC);
+                    in = (cy / T::YC) == ch;
+                    a = z, b = cx + TX * (cy - ch * T::YC);
                 } else {
-                    in = (z / C::ZC) == ch;
+                    in = m == ch;
                     a = DIR == 0 ? cx : cy;
-                    b = (DIR == 0 ? cy : cx) + SW::C1 * (z - ch * C::ZC);
+                    b = (DIR == 0 ? cy + TY * cz0 : cx + TX * cz0);
                 }
                 if (in) {
-                    const int f0 = a + (SW::L + 1) * b;
+                    const int f0 = a + (LEN + 1) * b;
 #pragma unroll
-                    for (int n = 0; n < C::VG; ++n)
-                        acc[m][n] += double(sG[n * C::NFMAX + f0]) - double(sG[n * C::NFMAX + f0 + 1]);
+                    for (int n = 0; n < L::VG; ++n)
+                        acc[m][n] += double(sG[n * L::NFMAX + f0]) - double(sG[n * L::NFMAX + f0 + 1]);
                 }
             }
             __syncthreads();
@@ -445,29 +445,27 @@ struct Tile {
     // ---------------------------------------------------------------- epilogue
     // The accumulators leave registers through shared memory so the (not unrolled) cell loop
     // below does not force them into local memory for the whole kernel.
-    __device__ void epilogue(const double (&acc)[CPT][C::VG]) {
+    __device__ void epilogue(const double (&acc)[CPT][L::VG]) {
         const int tid = threadIdx.x;
-        __syncthreads();  // every thread is done reading the working arrays
         double *sAcc = reinterpret_cast<double *>(sPhi);
 #pragma unroll
         for (int m = 0; m < CPT; ++m)
 #pragma unroll
-            for (int n = 0; n < C::VG; ++n) sAcc[(m * C::VG + n) * NT + tid] = acc[m][n];
+            for (int n = 0; n < L::VG; ++n) sAcc[(m * L::VG + n) * NT + tid] = acc[m][n];
         const int cx = tid % TX, cy = (tid / TX) % TY, cz0 = tid / (TX * TY);
-        const Dims &D = A.D;
+        const int np = A.np, ng = A.ng;
 #pragma unroll 1
         for (int m = 0; m < CPT; ++m) {
-            const int cz = cz0 + 2 * m;
-            const long long ix = X0 + cx, iy = Y0 + cy, iz = Z0 + cz;
-            if (ix >= D.nx || iy >= D.ny || iz >= D.nz) continue;
-            const long long g = (ix + D.ng) + sy * ((iy + D.ng) + D.ty * (iz + D.ng));
-            const double Jact = A.m.J[g] * A.dt;
+            const int ix = X0 + cx, iy = Y0 + cy, iz = Z0 + cz0 + T::ZC * m;
+            if (ix >= A.nx || iy >= A.ny || iz >= A.nz) continue;
+            const int g = (ix + ng) + A.sy * (iy + ng) + A.sz * (iz + ng);
+            const double Jact = A.met[9][g] * A.dt;
             double Uc[5], r[NS];
 #pragma unroll
             for (int n = 0; n < 5; ++n) {
                 const double u0 = A.U[g + n * np];
                 if (A.stage == 1) A.Un[g + n * np] = u0;
-                double un = u0 + sAcc[(m * C::VG + n) * NT + tid] * Jact;
+                double un = u0 + sAcc[(m * L::VG + n) * NT + tid] * Jact;
                 if (A.stage > 1) un = un * A.ca + A.Un[g + n * np] * A.cb;
                 Uc[n] = un;
                 A.U[g + n * np] = un;
@@ -476,7 +474,7 @@ struct Tile {
             for (int n = 0; n < NS; ++n) {
                 const double r0 = A.ri[g + n * np];
                 if (A.stage == 1) A.rn[g + n * np] = r0;
-                double rv = r0 + sAcc[(m * C::VG + 5 + n) * NT + tid] * Jact;
+                double rv = r0 + sAcc[(m * L::VG + 5 + n) * NT + tid] * Jact;
                 if (A.stage > 1) rv = rv * A.ca + A.rn[g + n * np] * A.cb;
                 r[n] = rv;
             }
@@ -491,23 +489,28 @@ struct Tile {
             for (int n = 0; n < NS; ++n) r[n] *= sc;
             const double u = Uc[1] * rinv, v = Uc[2] * rinv, w = Uc[3] * rinv;
             const double ei = jmax(Uc[4] - 0.5 * rho * (u * u + v * v + w * w), kEps);
-            const double T = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
-            const double p = jmax(p_mixture<NS>(A.th, NS, T, r), kEps);
-            const double qv[7] = {rho, u, v, w, p, T, ei};
+            const double Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
+            const double p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
+            double mu, lam, D;
+            transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
+            const double qv[7] = {rho, u, v, w, p, Tn, ei};
+            const double tv[3] = {mu, lam, D};
             // the cell and its periodic ghost images (new: the reference fills ghosts with
             // case-specific kernels, boundary.jl:1-191)
-            const long long gx = ix + D.ng, gy = iy + D.ng, gz = iz + D.ng;
-            long long ox[2] = {0, 0}, oy[2] = {0, 0}, oz[2] = {0, 0};
+            const int gx = ix + ng, gy = iy + ng, gz = iz + ng;
+            int ox[2] = {0, 0}, oy[2] = {0, 0}, oz[2] = {0, 0};
             int nxo = 1, nyo = 1, nzo = 1;
-            if (gx < 2 * D.ng) ox[nxo++] = D.nx; else if (gx >= D.nx) ox[nxo++] = -D.nx;
-            if (gy < 2 * D.ng) oy[nyo++] = D.ny; else if (gy >= D.ny) oy[nyo++] = -D.ny;
-            if (gz < 2 * D.ng) oz[nzo++] = D.nz; else if (gz >= D.nz) oz[nzo++] = -D.nz;
+            if (gx < 2 * ng) ox[nxo++] = A.nx; else if (gx >= A.nx) ox[nxo++] = -A.nx;
+            if (gy < 2 * ng) oy[nyo++] = A.ny; else if (gy >= A.ny) oy[nyo++] = -A.ny;
+            if (gz < 2 * ng) oz[nzo++] = A.nz; else if (gz >= A.nz) oz[nzo++] = -A.nz;
             for (int c = 0; c < nzo; ++c)
                 for (int b = 0; b < nyo; ++b)
                     for (int a = 0; a < nxo; ++a) {
-                        const long long t = (gx + ox[a]) + sy * ((gy + oy[b]) + D.ty * (gz + oz[c]));
+                        const int t = (gx + ox[a]) + A.sy * (gy + oy[b]) + A.sz * (gz + oz[c]);
 #pragma unroll
                         for (int n = 0; n < 7; ++n) A.Qo[t + n * np] = QT(qv[n]);
+#pragma unroll
+                        for (int n = 0; n < 3; ++n) A.To[t + n * np] = QT(tv[n]);
 #pragma unroll
                         for (int n = 0; n < NS; ++n) A.ro[t + n * np] = r[n];
                     }
@@ -515,61 +518,91 @@ struct Tile {
     }
 };
 
-template <int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(NT, 1) k_stage(const __grid_constant__ Args<QT> A) {
+template <class T, int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Tile<NS, QT, CT> t(A, reinterpret_cast<CT *>(smem_raw));
-    double acc[CPT][Cfg<NS>::VG];
+    Tile<T, NS, QT, CT> t(A, reinterpret_cast<CT *>(smem_raw));
+    double acc[T::CPT][Layout<T, NS>::VG];
 #pragma unroll
-    for (int m = 0; m < CPT; ++m)
+    for (int m = 0; m < T::CPT; ++m)
 #pragma unroll
-        for (int n = 0; n < Cfg<NS>::VG; ++n) acc[m][n] = 0.0;
+        for (int n = 0; n < Layout<T, NS>::VG; ++n) acc[m][n] = 0.0;
     t.point_phase();
     __syncthreads();
     t.template sweep<0>(acc);
     t.template sweep<1>(acc);
     t.template sweep<2>(acc);
+    __syncthreads();  // every thread is done with the working arrays before the hand-off
     t.epilogue(acc);
 }
 
-template <int NS, typename QT, typename CT>
-int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const FlameStageBuffers &b,
-           const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr) {
+// Transport of every ghosted point of a state (used once to start the fused stage loop).
+template <int NS, typename QT>
+__global__ void k_transport(int np, const QT *__restrict__ Q, const double *__restrict__ ri,
+                            QT *__restrict__ To, const FlameThermo th, const FlameTransport tr) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    double r[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) r[n] = ri[c + n * np];
+    double mu, lam, D;
+    transport_point<NS>(th, tr, double(Q[c + 5 * np]), double(Q[c]), r, mu, lam, D);
+    To[c] = QT(mu), To[c + np] = QT(lam), To[c + 2 * np] = QT(D);
+}
+
+template <typename QT>
+Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuffers &b,
+                   const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr) {
     Args<QT> A;
-    A.D = make_dims(g);
+    A.nx = g.nx, A.ny = g.ny, A.nz = g.nz, A.ng = g.ng;
+    A.tx = g.nx + 2 * g.ng, A.ty = g.ny + 2 * g.ng, A.tz = g.nz + 2 * g.ng;
+    A.np = A.tx * A.ty * A.tz;
+    A.sy = A.tx, A.sz = A.tx * A.ty;
     A.stage = stage;
     A.dt = dt;
     A.ca = stage == 2 ? 0.25 : 2.0 / 3.0;
     A.cb = stage == 2 ? 0.75 : 1.0 / 3.0;
     A.U = b.U, A.Un = b.Un;
-    A.Qi = reinterpret_cast<const QT *>(b.Q_in);
-    A.Qo = reinterpret_cast<QT *>(b.Q_out);
+    A.Qi = static_cast<const QT *>(b.Q_in);
+    A.Qo = static_cast<QT *>(b.Q_out);
+    A.Ti = static_cast<const QT *>(b.trans_in);
+    A.To = static_cast<QT *>(b.trans_out);
     A.ri = b.rhoi_in, A.ro = b.rhoi_out, A.rn = b.rhon;
-    A.m = m, A.th = th, A.tr = tr;
-    constexpr size_t sm = smem_bytes<NS, CT>();
+    const double *mm[10] = {m.dxidx,   m.dxidy,   m.dxidz,   m.detadx, m.detady,
+                            m.detadz,  m.dzetadx, m.dzetady, m.dzetadz, m.J};
+    for (int i = 0; i < 10; ++i) A.met[i] = mm[i];
+    A.th = th, A.tr = tr;
+    return A;
+}
+
+template <class T, int NS, typename QT, typename CT>
+int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const FlameStageBuffers &b,
+           const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr) {
+    const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr);
+    constexpr size_t sm = smem_bytes<T, NS, CT>();
     static bool attr_set[64] = {};  // the attribute is per function and device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(
-            k_stage<NS, QT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = cudaFuncSetAttribute(k_stage<T, NS, QT, CT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess)
             return flame_fail(FLAME_ELAUNCH, "flame_rk_stage: %zu B shared memory: %s", sm,
                               cudaGetErrorString(e));
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
-    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + TZ - 1) / TZ);
-    k_stage<NS, QT, CT><<<grid, NT, sm, s>>>(A);
+    dim3 grid((g.nx + T::TX - 1) / T::TX, (g.ny + T::TY - 1) / T::TY, (g.nz + T::TZ - 1) / T::TZ);
+    k_stage<T, NS, QT, CT><<<grid, T::NT, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage");
 }
 
-template <typename QT, typename CT>
-int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
-             const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
-             const FlameTransport &tr) {
+template <class T, typename QT, typename CT>
+int dispatch_ns(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
+                const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
+                const FlameTransport &tr) {
     switch (ns) {
 #define CASE(N) \
-    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr);
+    case N: return launch<T, N, QT, CT>(g, s, stage, dt, b, m, th, tr);
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
         default:
@@ -578,15 +611,78 @@ int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
     }
 }
 
+template <typename QT, typename CT>
+int dispatch_tile(int tile, int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
+                  const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
+                  const FlameTransport &tr) {
+    switch (tile) {
+        case 0: return dispatch_ns<Cfg16x8x8, QT, CT>(ns, g, s, stage, dt, b, m, th, tr);
+        case 1: return dispatch_ns<Cfg16x8x8b2, QT, CT>(ns, g, s, stage, dt, b, m, th, tr);
+        case 2: return dispatch_ns<Cfg8x8x8, QT, CT>(ns, g, s, stage, dt, b, m, th, tr);
+        case 3:
+            return flame_pencil_stage(&g, s, stage, dt, &b, &m, &th, &tr,
+                                      sizeof(QT) == 8 ? 0 : 1, b.scratch);
+        default: return flame_fail(FLAME_EINVAL, "flame_rk_stage: tile config %d unknown", tile);
+    }
+}
+
+template <typename QT>
+int transport_ns(int ns, int np, cudaStream_t s, const void *Q, const double *ri, void *To,
+                 const FlameThermo &th, const FlameTransport &tr) {
+    const unsigned blocks = (unsigned)((np + 255) / 256);
+    const QT *q = static_cast<const QT *>(Q);
+    QT *t = static_cast<QT *>(To);
+    switch (ns) {
+#define CASE(N) \
+    case N: k_transport<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr); break;
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
+#undef CASE
+        default: return flame_fail(FLAME_EUNSUPPORTED, "flame_transport: ns=%d", ns);
+    }
+    return flame_check_launch("flame_transport");
+}
+
 }  // namespace fused
 }  // namespace flame
 
-extern "C" int flame_rk_stage(const FlameGrid *g, flame_stream_t s, int stage, double dt,
-                              const FlameStageBuffers *b, const FlameMetrics *m,
-                              const FlameThermo *th, const FlameTransport *tr, int precision) {
+namespace {
+int check_sizes(const FlameGrid *g, const char *what) {
+    const long long np = (long long)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
+    const long long nv = g->ns > 10 ? g->ns : 10;
+    if (np * nv >= (1LL << 31))
+        return flame_fail(FLAME_EINVAL, "%s: %lld points x %lld fields exceeds 2^31 elements", what,
+                          np, nv);
+    return FLAME_OK;
+}
+}  // namespace
+
+extern "C" int flame_transport(const FlameGrid *g, flame_stream_t s, const void *Q,
+                               const double *rhoi, void *trans, const FlameThermo *th,
+                               const FlameTransport *tr, int precision) {
+    if (int e = flame_check_grid(g, "flame_transport")) return e;
+    if (int e = check_sizes(g, "flame_transport")) return e;
+    if (!Q || !rhoi || !trans || !th || !tr)
+        return flame_fail(FLAME_EINVAL, "flame_transport: NULL argument");
+    if (tr->law != 0 && tr->law != 1)
+        return flame_fail(FLAME_EINVAL, "flame_transport: transport law %d unknown", tr->law);
+    const int np = (g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
+    if (precision == 0)
+        return flame::fused::transport_ns<double>(g->ns, np, s, Q, rhoi, trans, *th, *tr);
+    if (precision == 1)
+        return flame::fused::transport_ns<float>(g->ns, np, s, Q, rhoi, trans, *th, *tr);
+    return flame_fail(FLAME_EINVAL, "flame_transport: precision=%d must be 0 or 1", precision);
+}
+
+extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int stage, double dt,
+                                    const FlameStageBuffers *b, const FlameMetrics *m,
+                                    const FlameThermo *th, const FlameTransport *tr,
+                                    int precision, int tile) {
     if (int e = flame_check_grid(g, "flame_rk_stage")) return e;
+    if (int e = check_sizes(g, "flame_rk_stage")) return e;
     if (!b || !m || !th || !tr || !b->U || !b->Un || !b->Q_in || !b->Q_out || !b->rhoi_in ||
-        !b->rhoi_out || !b->rhon || !m->J || !m->dxidx || !m->dzetadz)
+        !b->rhoi_out || !b->rhon || !b->trans_in || !b->trans_out || !m->J || !m->dxidx ||
+        !m->dxidy || !m->dxidz || !m->detadx || !m->detady || !m->detadz || !m->dzetadx ||
+        !m->dzetady || !m->dzetadz)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: NULL argument");
     if (stage < 1 || stage > 3)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: stage=%d must be 1, 2 or 3", stage);
@@ -596,14 +692,22 @@ extern "C" int flame_rk_stage(const FlameGrid *g, flame_stream_t s, int stage, d
                           "use the per-kernel entry points with the case's own ghost fill");
     if (g->nx < FLAME_NG || g->ny < FLAME_NG || g->nz < FLAME_NG)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: extents must be >= %d", FLAME_NG);
-    if ((const void *)b->Q_in == (const void *)b->Q_out ||
-        (const void *)b->rhoi_in == (const void *)b->rhoi_out)
+    if (b->Q_in == b->Q_out || (const void *)b->rhoi_in == (const void *)b->rhoi_out ||
+        b->trans_in == b->trans_out)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: in and out buffers must differ");
     if (tr->law != 0 && tr->law != 1)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: transport law %d unknown", tr->law);
     if (precision == 0)
-        return flame::fused::dispatch<double, double>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr);
+        return flame::fused::dispatch_tile<double, double>(tile, g->ns, *g, s, stage, dt, *b, *m,
+                                                           *th, *tr);
     if (precision == 1)
-        return flame::fused::dispatch<float, float>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr);
+        return flame::fused::dispatch_tile<float, float>(tile, g->ns, *g, s, stage, dt, *b, *m,
+                                                         *th, *tr);
     return flame_fail(FLAME_EINVAL, "flame_rk_stage: precision=%d must be 0 or 1", precision);
+}
+
+extern "C" int flame_rk_stage(const FlameGrid *g, flame_stream_t s, int stage, double dt,
+                              const FlameStageBuffers *b, const FlameMetrics *m,
+                              const FlameThermo *th, const FlameTransport *tr, int precision) {
+    return flame_rk_stage_tiled(g, s, stage, dt, b, m, th, tr, precision, 0);
 }

@@ -1,0 +1,533 @@
+// pencil_stage.cu — the RK3 stage as four barrier-free sweeps (sm_100a).
+//
+// One stage of solver.jl:298-326 on a periodic grid, organised for latency hiding instead of
+// shared-memory tiling:
+//   k_prep      every ghosted point: shock sensor ϕ (schemes.jl:1-24) and the mass fractions
+//               Y = max(ρi / max(ρ, eps), 0) (thermo.jl:391-394) into a scratch array;
+//   k_pencil<2> z sweep, k_pencil<1> y sweep, k_pencil<0> x sweep: a warp owns a pencil of 32
+//               points along the sweep axis (26 owned cells plus the 3 + 3 stencil halo).  Each
+//               lane splits its point once (split.jl:17-130), computes the cell-centred
+//               tangential derivatives the viscous fluxes average across a face, and publishes
+//               everything in the warp's slice of shared memory; the face between lanes l-1 and
+//               l then forms the hybrid UP7 / WENO-Z / minmod flux (schemes.jl:86-437) minus the
+//               viscous and species-diffusion flux (viscous.jl:1-665); the difference of two
+//               faces is the cell's contribution.  Only __syncwarp orders the phases.
+//   The z and y sweeps accumulate into a scratch right-hand side; the x sweep (lanes along x,
+//   so its stores coalesce) finishes the stage: div (div.jl), RK3 combination (utils.jl:95-112),
+//   c2Prim with the Newton temperature (utils.jl:2-48, thermo.jl:231-282), the transport law of
+//   the new state, and the periodic ghost images.
+//
+// Template parameters as in fused_stage.cu: NS species, QT storage of Q / transport, CT
+// arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
+
+#include "common.cuh"
+
+namespace flame {
+namespace pencil {
+
+constexpr int OWN = 26;  // cells owned by a 32-lane pencil (3 halo lanes below, 3 above)
+
+// Warps per block.  The x sweep reads whole rows per warp; the y and z sweeps read one value per
+// lane from 32 different rows, so their blocks take 16 consecutive x columns and together use
+// every byte of each 128-byte line they touch.
+template <int DIR>
+struct Wpb {
+    static constexpr int value = DIR == 0 ? 4 : 16;
+};
+
+template <typename QT>
+struct Args {
+    int nx, ny, nz, ng, tx, ty, tz, np, sy, sz;
+    int stage;
+    double dt, ca, cb;
+    double *U, *Un;
+    const QT *Qi;
+    QT *Qo;
+    const QT *Ti;
+    QT *To;
+    const double *ri;
+    double *ro, *rn;
+    const double *met[10];
+    QT *aux;     // ϕ (1) and Y (NS), ghosted
+    double *R;   // right-hand side accumulator (5 + NS), ghosted indexing
+    FlameThermo th;
+    FlameTransport tr;
+};
+
+// Shared-memory slots of one lane's point (CT each).
+template <int NS>
+struct Slots {
+    static constexpr int FP = 0;                // F+ flow (5), F- flow (5), F+ sp (NS), F- sp (NS)
+    static constexpr int VF = 10 + 2 * NS;
+    static constexpr int Q4 = VF;               // u v w T
+    static constexpr int MET = Q4 + 4;          // 9 metrics + J
+    static constexpr int TR = MET + 10;         // μ λ D
+    static constexpr int RHO = TR + 3;
+    static constexpr int Y = RHO + 1;           // NS
+    static constexpr int DQ1 = Y + NS;          // tangential derivatives of u v w T along d+1
+    static constexpr int DQ2 = DQ1 + 4;         // ... along d+2
+    static constexpr int DY1 = DQ2 + 4;         // Y[+] - Y[-] along d+1 (NS)
+    static constexpr int DY2 = DY1 + NS;        // ... along d+2 (NS)
+    static constexpr int PHI = DY2 + NS;
+    static constexpr int N = PHI + 1;
+    static constexpr int G = FP;                // face flux, reuses the split slots (5 + NS)
+};
+
+template <int NS, typename CT, int WPB>
+constexpr size_t smem_bytes() {
+    return sizeof(CT) * Slots<NS>::N * 32 * WPB;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+template <typename CT, typename T>
+__device__ __forceinline__ CT ldg(const T *p, int i) {
+    return CT(__ldg(p + i));
+}
+
+// ----------------------------------------------------------------------------------- prep
+template <int NS, typename QT>
+__global__ void __launch_bounds__(256) k_prep(const __grid_constant__ Args<QT> A) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.np) return;
+    const int gx = c % A.tx, gy = (c / A.tx) % A.ty, gz = c / A.sz;
+    const QT *P = A.Qi + 4 * A.np;
+    double phi = 0;
+    if (gx > 0 && gx < A.tx - 1 && gy > 0 && gy < A.ty - 1 && gz > 0 && gz < A.tz - 1) {
+        // schemes.jl:10-22 in the arithmetic type of Q with exact divisions, so the branch
+        // thresholds see the same ϕ as the reference
+        using CT = QT;
+        const CT P2 = P[c];
+        CT a1 = P[c - 1], a3 = P[c + 1];
+        const CT phx = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+        a1 = P[c - A.sy], a3 = P[c + A.sy];
+        const CT phy = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+        a1 = P[c - A.sz], a3 = P[c + A.sz];
+        const CT phz = fabs(-a1 + 2 * P2 - a3) / (a1 + 2 * P2 + a3);
+        phi = phx + phy + phz;
+    }
+    A.aux[c] = QT(phi);
+    const double rinv = 1 / jmax(double(A.Qi[c]), kEps);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) A.aux[c + (1 + n) * A.np] = QT(jmax(A.ri[c + n * A.np] * rinv, 0.0));
+}
+
+// ----------------------------------------------------------------------------------- sweep
+template <int DIR>
+struct Dir {
+    static constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
+};
+
+template <int NS>
+__device__ __forceinline__ void transport_point(const FlameThermo &th, const FlameTransport &tr,
+                                                double T, double rho_raw, const double *r,
+                                                double &mu, double &lam, double &D) {
+    if (tr.law == 0) {
+        mu = tr.mu_ref, lam = tr.lambda_ref, D = tr.D_ref;
+        return;
+    }
+    const double rho = jmax(rho_raw, kEps);
+    const double rinv = 1 / rho;
+    const double T2 = T * T, T3 = T2 * T, T4 = T2 * T2;
+    double cpm = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n)
+        cpm += cp_spec(th, n, T, T2, T3, T4) * jmax(r[n] * rinv, 0.0) / th.mw[n];
+    cpm *= th.Ru;
+    mu = tr.mu_ref * pow(T / tr.T_ref, tr.exponent);
+    lam = cpm * mu / tr.Pr;
+    D = lam / (rho * cpm);
+}
+
+// PASS: 0 = first sweep (writes R), 1 = middle (adds to R), 2 = last (finishes the stage).
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Wpb<DIR>::value * 32) k_pencil(const __grid_constant__ Args<QT> A) {
+    constexpr int WPB = Wpb<DIR>::value;
+    using SL = Slots<NS>;
+    constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    CT *S = reinterpret_cast<CT *>(smem_raw) + warp * SL::N * 32;
+#define SV(slot, l) S[(slot) * 32 + (l)]
+
+    // ---- which pencil: warps of a block take consecutive cross-x positions for y/z sweeps
+    const int n_along = DIR == 0 ? A.nx : (DIR == 1 ? A.ny : A.nz);
+    const int nseg = (n_along + OWN - 1) / OWN;
+    const int gw = blockIdx.x * WPB + warp;
+    int seg, c1, c2;  // c1, c2: interior cross coordinates
+    if (DIR == 0) {
+        seg = gw % nseg;
+        const int r = gw / nseg;
+        c1 = r % A.ny, c2 = r / A.ny;  // y, z
+        if (c2 >= A.nz) return;
+    } else {
+        c1 = gw % A.nx;  // x
+        const int r = gw / A.nx;
+        seg = r % nseg;
+        c2 = r / nseg;  // z for DIR 1, y for DIR 2
+        if (c2 >= (DIR == 1 ? A.nz : A.ny)) return;
+    }
+    const int a = seg * OWN - 3 + lane;                    // interior along-coordinate
+    const int ga = clampi(a + A.ng, 0, n_along + 2 * A.ng - 1);  // ghosted, kept in the array
+    int gx, gy, gz;
+    if (DIR == 0) gx = ga, gy = c1 + A.ng, gz = c2 + A.ng;
+    else if (DIR == 1) gx = c1 + A.ng, gy = ga, gz = c2 + A.ng;
+    else gx = c1 + A.ng, gy = c2 + A.ng, gz = ga;
+    const int g = gx + A.sy * gy + A.sz * gz;
+    const int np = A.np;
+    const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
+    const int s2 = D2 == 0 ? 1 : (D2 == 1 ? A.sy : A.sz);
+    const QT *Q = A.Qi;
+    const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
+
+    // ---- phase A: this lane's point
+    {
+        const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]),
+                 p = CT(Q[g + 4 * np]), T = CT(Q[g + 5 * np]), ei = CT(Q[g + 6 * np]);
+        CT A1 = ldg<CT>(A.met[3 * DIR], g), A2 = ldg<CT>(A.met[3 * DIR + 1], g),
+           A3 = ldg<CT>(A.met[3 * DIR + 2], g);
+        // Steger-Warming split, split.jl:17-89 (divisions folded into reciprocals)
+        {
+            const CT gam = p * (CT(1) / ei) + 1;
+            const CT gm1 = gam - 1;
+            const CT inv = CT(1) / (rho * gam * gm1);
+            const CT cs = sqrt(gam * p * (gam * gm1 * inv));
+            const CT r2 = A1 * A1 + A2 * A2 + A3 * A3;
+            const CT rs = rsqrt(r2);
+            const CT ss = r2 * rs;
+            const CT E1 = A1 * u + A2 * v + A3 * w;
+            const CT E2 = E1 - cs * ss, E3 = E1 + cs * ss;
+            const CT B1 = A1 * rs, B2 = A2 * rs, B3 = A3 * rs;
+            const CT E1P = (E1 + fabs(E1)) * h, E2P = (E2 + fabs(E2)) * h, E3P = (E3 + fabs(E3)) * h;
+            const CT E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
+            const CT uc1 = u - cs * B1, uc2 = u + cs * B1;
+            const CT vc1 = v - cs * B2, vc2 = v + cs * B2;
+            const CT wc1 = w - cs * B3, wc2 = w + cs * B3;
+            const CT vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * h;
+            const CT vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * h;
+            const CT vv = gm1 * (u * u + v * v + w * w);
+            const CT W2 = (3 - gam) * (h * rho * gam * inv) * (cs * cs);
+            const CT tmp1 = h * rho * (rho * gm1 * inv);
+            const CT tmp2 = 2 * gm1;
+            SV(0, lane) = tmp1 * (tmp2 * E1P + E2P + E3P);
+            SV(1, lane) = tmp1 * (tmp2 * E1P * u + E2P * uc1 + E3P * uc2);
+            SV(2, lane) = tmp1 * (tmp2 * E1P * v + E2P * vc1 + E3P * vc2);
+            SV(3, lane) = tmp1 * (tmp2 * E1P * w + E2P * wc1 + E3P * wc2);
+            SV(4, lane) = tmp1 * (E1P * vv + E2P * vvc1 + E3P * vvc2 + W2 * (E2P + E3P));
+            SV(5, lane) = tmp1 * (tmp2 * E1M + E2M + E3M);
+            SV(6, lane) = tmp1 * (tmp2 * E1M * u + E2M * uc1 + E3M * uc2);
+            SV(7, lane) = tmp1 * (tmp2 * E1M * v + E2M * vc1 + E3M * vc2);
+            SV(8, lane) = tmp1 * (tmp2 * E1M * w + E2M * wc1 + E3M * wc2);
+            SV(9, lane) = tmp1 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
+            // species, split.jl:101-130
+            const CT Ep = h * (E1 + fabs(E1)), Em = h * (E1 - fabs(E1));
+#pragma unroll
+            for (int n = 0; n < NS; ++n) {
+                const CT r = CT(A.ri[g + n * np]);
+                SV(10 + n, lane) = Ep * r;
+                SV(10 + NS + n, lane) = Em * r;
+            }
+        }
+        SV(SL::Q4 + 0, lane) = u, SV(SL::Q4 + 1, lane) = v, SV(SL::Q4 + 2, lane) = w;
+        SV(SL::Q4 + 3, lane) = T;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) SV(SL::MET + m, lane) = ldg<CT>(A.met[m], g);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) SV(SL::TR + m, lane) = CT(A.Ti[g + m * np]);
+        SV(SL::RHO, lane) = rho;
+        SV(SL::PHI, lane) = CT(A.aux[g]);
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            const QT *Y = A.aux + (1 + n) * np;
+            SV(SL::Y + n, lane) = CT(Y[g]);
+            SV(SL::DY1 + n, lane) = CT(Y[g + s1]) - CT(Y[g - s1]);
+            SV(SL::DY2 + n, lane) = CT(Y[g + s2]) - CT(Y[g - s2]);
+        }
+        // cell-centred 4th-order tangential derivatives of u, v, w, T; the face value the
+        // reference forms (viscous.jl:36-53) is the mean of the two cells' values
+        const int qv[4] = {1, 2, 3, 5};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const QT *q = Q + qv[m] * np + g;
+            SV(SL::DQ1 + m, lane) = c23 * (CT(q[s1]) - CT(q[-s1])) - c12 * (CT(q[2 * s1]) - CT(q[-2 * s1]));
+            SV(SL::DQ2 + m, lane) = c23 * (CT(q[s2]) - CT(q[-s2])) - c12 * (CT(q[2 * s2]) - CT(q[-2 * s2]));
+        }
+    }
+    __syncwarp();
+
+    // ---- phase B: face between lanes l-1 and l (faces of the owned cells and one more)
+    CT G[5 + NS];
+    const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
+    if (face) {
+        const int l = lane, lm = lane - 1;
+        const CT phif = CT(jmax(double(SV(SL::PHI, lm)), double(SV(SL::PHI, l))));
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) {
+            const int vp = n < 5 ? n : 5 + n;
+            const int vm = n < 5 ? 5 + n : 5 + NS + n;
+            CT pv[7], mv[7];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) pv[i] = SV(vp, l - 3 + i), mv[i] = SV(vm, l - 3 + i);
+            pv[6] = mv[6] = CT(0);
+            G[n] = hybrid_face7<CT>(pv, mv, phif);
+        }
+        CT met[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) met[m] = (SV(SL::MET + m, lm) + SV(SL::MET + m, l)) * h;
+        const CT Jac = (SV(SL::MET + 9, lm) + SV(SL::MET + 9, l)) * h;
+        const CT mui = (SV(SL::TR, lm) + SV(SL::TR, l)) * h;
+        const CT lami = (SV(SL::TR + 1, lm) + SV(SL::TR + 1, l)) * h;
+        const CT DL = SV(SL::TR + 2, lm), DR = SV(SL::TR + 2, l);
+        const CT rho = (SV(SL::RHO, lm) + SV(SL::RHO, l)) * h;
+        const CT Tf = (SV(SL::Q4 + 3, lm) + SV(SL::Q4 + 3, l)) * h;
+        const CT *md = met + 3 * DIR;
+        // species diffusion (viscous.jl:430-507) first: it yields Fh for the energy flux
+        CT Vk1[NS], Vk2[NS], Vk3[NS], Yf[NS];
+        CT sum1 = 0, sum2 = 0, sum3 = 0;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            const CT y0 = SV(SL::Y + n, l), ym = SV(SL::Y + n, lm);
+            const CT yp = SV(SL::Y + n, l + 1), ymm = SV(SL::Y + n, l - 2);
+            CT dY[3];
+            dY[DIR] = CT(1.25) * (y0 - ym) - c12 * (yp - ymm);
+            dY[D1] = CT(0.25) * (SV(SL::DY1 + n, l) + SV(SL::DY1 + n, lm));
+            dY[D2] = CT(0.25) * (SV(SL::DY2 + n, l) + SV(SL::DY2 + n, lm));
+            const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
+            const CT Vx = (dY[0] * met[0] + dY[1] * met[3] + dY[2] * met[6]) * Jac * rhoDi;
+            const CT Vy = (dY[0] * met[1] + dY[1] * met[4] + dY[2] * met[7]) * Jac * rhoDi;
+            const CT Vz = (dY[0] * met[2] + dY[1] * met[5] + dY[2] * met[8]) * Jac * rhoDi;
+            Vk1[n] = Vx, Vk2[n] = Vy, Vk3[n] = Vz;
+            sum1 += Vx, sum2 += Vy, sum3 += Vz;
+            Yf[n] = h * (ym + y0);
+        }
+        CT fh1 = 0, fh2 = 0, fh3 = 0;
+        {
+            const double Td = double(Tf);
+            const double T2 = 0.5 * Td * Td, T3 = 2.0 / 3.0 * T2 * Td, T4 = T2 * T2,
+                         T5 = 0.8 * T4 * Td;
+#pragma unroll
+            for (int n = 0; n < NS; ++n) {
+                const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
+                const CT V1 = Vk1[n] - sum1 * Yf[n], V2 = Vk2[n] - sum2 * Yf[n],
+                         V3 = Vk3[n] - sum3 * Yf[n];
+                G[5 + n] -= V1 * md[0] + V2 * md[1] + V3 * md[2];
+                fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
+            }
+        }
+        // momentum and energy, viscous.jl:14-141
+        CT gr[4][3];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            CT dq[3];
+            dq[DIR] = CT(1.25) * (SV(SL::Q4 + m, l) - SV(SL::Q4 + m, lm)) -
+                      c12 * (SV(SL::Q4 + m, l + 1) - SV(SL::Q4 + m, l - 2));
+            dq[D1] = h * (SV(SL::DQ1 + m, l) + SV(SL::DQ1 + m, lm));
+            dq[D2] = h * (SV(SL::DQ2 + m, l) + SV(SL::DQ2 + m, lm));
+#pragma unroll
+            for (int x = 0; x < 3; ++x)
+                gr[m][x] = (dq[0] * met[x] + dq[1] * met[3 + x] + dq[2] * met[6 + x]) * Jac;
+        }
+        const CT u = (SV(SL::Q4 + 0, lm) + SV(SL::Q4 + 0, l)) * h;
+        const CT v = (SV(SL::Q4 + 1, lm) + SV(SL::Q4 + 1, l)) * h;
+        const CT w = (SV(SL::Q4 + 2, lm) + SV(SL::Q4 + 2, l)) * h;
+        const CT div = gr[0][0] + gr[1][1] + gr[2][2];
+        const CT t11 = mui * (2 * gr[0][0] - c23 * div);
+        const CT t12 = mui * (gr[0][1] + gr[1][0]);
+        const CT t13 = mui * (gr[0][2] + gr[2][0]);
+        const CT t22 = mui * (2 * gr[1][1] - c23 * div);
+        const CT t23 = mui * (gr[2][1] + gr[1][2]);
+        const CT t33 = mui * (2 * gr[2][2] - c23 * div);
+        const CT E1 = u * t11 + v * t12 + w * t13 + lami * gr[3][0] + fh1;
+        const CT E2 = u * t12 + v * t22 + w * t23 + lami * gr[3][1] + fh2;
+        const CT E3 = u * t13 + v * t23 + w * t33 + lami * gr[3][2] + fh3;
+        G[1] -= md[0] * t11 + md[1] * t12 + md[2] * t13;
+        G[2] -= md[0] * t12 + md[1] * t22 + md[2] * t23;
+        G[3] -= md[0] * t13 + md[1] * t23 + md[2] * t33;
+        G[4] -= md[0] * E1 + md[1] * E2 + md[2] * E3;
+    }
+    __syncwarp();
+    if (face) {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) SV(SL::G + n, lane) = G[n];
+    }
+    __syncwarp();
+
+    // ---- phase C: the owned cell of this lane
+    if (lane < 3 || lane >= 3 + OWN || a >= n_along) return;
+    double rhs[5 + NS];
+#pragma unroll
+    for (int n = 0; n < 5 + NS; ++n)
+        rhs[n] = double(SV(SL::G + n, lane)) - double(SV(SL::G + n, lane + 1));
+#undef SV
+    if (PASS == 0) {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * np] = rhs[n];
+        return;
+    }
+    if (PASS == 1) {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * np] += rhs[n];
+        return;
+    }
+    // last sweep: div, RK3 combination, c2Prim, transport, ghost images
+    const double Jact = A.met[9][g] * A.dt;
+    double Uc[5], r[NS];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+        const double u0 = A.U[g + n * np];
+        if (A.stage == 1) A.Un[g + n * np] = u0;
+        double un = u0 + (A.R[g + n * np] + rhs[n]) * Jact;
+        if (A.stage > 1) un = un * A.ca + A.Un[g + n * np] * A.cb;
+        Uc[n] = un;
+        A.U[g + n * np] = un;
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        const double r0 = A.ri[g + n * np];
+        if (A.stage == 1) A.rn[g + n * np] = r0;
+        double rv = r0 + (A.R[g + (5 + n) * np] + rhs[5 + n]) * Jact;
+        if (A.stage > 1) rv = rv * A.ca + A.rn[g + n * np] * A.cb;
+        r[n] = rv;
+    }
+    const double rho = jmax(Uc[0], kEps);
+    const double rinv = 1 / rho;
+    double sr = 0.0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) r[n] = jmax(r[n], 0.0), sr += r[n];
+    const double sc = rho / sr;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) r[n] *= sc;
+    const double u = Uc[1] * rinv, v = Uc[2] * rinv, w = Uc[3] * rinv;
+    const double ei = jmax(Uc[4] - 0.5 * rho * (u * u + v * v + w * w), kEps);
+    const double Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
+    const double p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
+    double mu, lam, D;
+    transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
+    const double qv[7] = {rho, u, v, w, p, Tn, ei};
+    const double tv[3] = {mu, lam, D};
+    const int ng = A.ng;
+    int ox[2] = {0, 0}, oy[2] = {0, 0}, oz[2] = {0, 0};
+    int nxo = 1, nyo = 1, nzo = 1;
+    if (gx < 2 * ng) ox[nxo++] = A.nx; else if (gx >= A.nx) ox[nxo++] = -A.nx;
+    if (gy < 2 * ng) oy[nyo++] = A.ny; else if (gy >= A.ny) oy[nyo++] = -A.ny;
+    if (gz < 2 * ng) oz[nzo++] = A.nz; else if (gz >= A.nz) oz[nzo++] = -A.nz;
+    for (int c = 0; c < nzo; ++c)
+        for (int b = 0; b < nyo; ++b)
+            for (int aa = 0; aa < nxo; ++aa) {
+                const int t = (gx + ox[aa]) + A.sy * (gy + oy[b]) + A.sz * (gz + oz[c]);
+#pragma unroll
+                for (int n = 0; n < 7; ++n) A.Qo[t + n * np] = QT(qv[n]);
+#pragma unroll
+                for (int n = 0; n < 3; ++n) A.To[t + n * np] = QT(tv[n]);
+#pragma unroll
+                for (int n = 0; n < NS; ++n) A.ro[t + n * np] = r[n];
+            }
+}
+
+template <typename QT>
+Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuffers &b,
+                   const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr,
+                   void *scratch) {
+    Args<QT> A;
+    A.nx = g.nx, A.ny = g.ny, A.nz = g.nz, A.ng = g.ng;
+    A.tx = g.nx + 2 * g.ng, A.ty = g.ny + 2 * g.ng, A.tz = g.nz + 2 * g.ng;
+    A.np = A.tx * A.ty * A.tz;
+    A.sy = A.tx, A.sz = A.tx * A.ty;
+    A.stage = stage;
+    A.dt = dt;
+    A.ca = stage == 2 ? 0.25 : 2.0 / 3.0;
+    A.cb = stage == 2 ? 0.75 : 1.0 / 3.0;
+    A.U = b.U, A.Un = b.Un;
+    A.Qi = static_cast<const QT *>(b.Q_in);
+    A.Qo = static_cast<QT *>(b.Q_out);
+    A.Ti = static_cast<const QT *>(b.trans_in);
+    A.To = static_cast<QT *>(b.trans_out);
+    A.ri = b.rhoi_in, A.ro = b.rhoi_out, A.rn = b.rhon;
+    const double *mm[10] = {m.dxidx,   m.dxidy,   m.dxidz,   m.detadx, m.detady,
+                            m.detadz,  m.dzetadx, m.dzetady, m.dzetadz, m.J};
+    for (int i = 0; i < 10; ++i) A.met[i] = mm[i];
+    // scratch: R (5 + NS doubles per point) first, then ϕ and Y (1 + NS of QT per point)
+    A.R = static_cast<double *>(scratch);
+    A.aux = reinterpret_cast<QT *>(A.R + (size_t)(5 + g.ns) * A.np);
+    A.th = th, A.tr = tr;
+    return A;
+}
+
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+int launch_sweep(const Args<QT> &A, cudaStream_t s) {
+    constexpr int WPB = Wpb<DIR>::value;
+    constexpr size_t sm = smem_bytes<NS, CT, WPB>();
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_pencil<DIR, PASS, NS, QT, CT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess)
+            return flame_fail(FLAME_ELAUNCH, "pencil sweep: %zu B shared memory: %s", sm,
+                              cudaGetErrorString(e));
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    const int n_along = DIR == 0 ? A.nx : (DIR == 1 ? A.ny : A.nz);
+    const int nseg = (n_along + OWN - 1) / OWN;
+    const long long cross = DIR == 0 ? (long long)A.ny * A.nz
+                                     : (long long)A.nx * (DIR == 1 ? A.nz : A.ny);
+    const long long warps = cross * nseg;
+    const unsigned blocks = (unsigned)((warps + WPB - 1) / WPB);
+    k_pencil<DIR, PASS, NS, QT, CT><<<blocks, WPB * 32, sm, s>>>(A);
+    return flame_check_launch("flame_rk_stage (pencil)");
+}
+
+template <int NS, typename QT, typename CT>
+int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const FlameStageBuffers &b,
+           const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr,
+           void *scratch) {
+    const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr, scratch);
+    k_prep<NS, QT><<<(unsigned)((A.np + 255) / 256), 256, 0, s>>>(A);
+    if (int e = flame_check_launch("flame_rk_stage (prep)")) return e;
+    if (int e = launch_sweep<2, 0, NS, QT, CT>(A, s)) return e;
+    if (int e = launch_sweep<1, 1, NS, QT, CT>(A, s)) return e;
+    return launch_sweep<0, 2, NS, QT, CT>(A, s);
+}
+
+template <typename QT, typename CT>
+int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
+             const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
+             const FlameTransport &tr, void *scratch) {
+    switch (ns) {
+#define CASE(N) \
+    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr, scratch);
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
+#undef CASE
+        default:
+            return flame_fail(FLAME_EUNSUPPORTED, "flame_rk_stage: ns=%d (pencil path has 1..9)",
+                              ns);
+    }
+}
+
+}  // namespace pencil
+}  // namespace flame
+
+// Entry used by fused_stage.cu's dispatcher for tile configuration 3.
+int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
+                       const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *th,
+                       const FlameTransport *tr, int precision, void *scratch) {
+    if (!scratch)
+        return flame_fail(FLAME_EINVAL,
+                          "flame_rk_stage: the pencil configuration needs scratch (see "
+                          "flame_stage_scratch_bytes)");
+    if (precision == 0)
+        return flame::pencil::dispatch<double, double>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
+                                                       scratch);
+    return flame::pencil::dispatch<float, float>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
+                                                 scratch);
+}
+
+extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
+    if (!g) return 0;
+    const size_t np = (size_t)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
+    const size_t q = precision == 0 ? sizeof(double) : sizeof(float);
+    return np * ((5 + g->ns) * sizeof(double) + (1 + g->ns) * q);
+}

@@ -32,7 +32,7 @@ class DeviceCase:
     """One case resident on one GPU."""
 
     def __init__(self, case: Case, device: str | torch.device = "cuda", precision: int = 0,
-                 sequence_buffers: bool = False):
+                 sequence_buffers: bool = False, tile: int | None = None):
         self.lib = abi.load_library()
         self.case = case
         self.device = torch.device(device)
@@ -62,10 +62,18 @@ class DeviceCase:
         self.U = torch.empty((5,) + shp, **f64)
         self.Un = torch.empty((5,) + shp, **f64)
         self.rhon = torch.empty((ns,) + shp, **f64)
+        # μ, λ, D of the state, recomputed by every fused stage for the next one
+        self.T = [torch.empty((3,) + shp, dtype=qdt, device=dev) for _ in range(2)]
         if precision == 0:
             self._call("flame_prim2c", _p(self.U), _p(self.Q[0]))
         else:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
+        self._transport()
+        self.tile = 0 if tile is None else tile
+        self.scratch = None
+        if self.tile == 3:
+            nbytes = self.lib.flame_stage_scratch_bytes(C.byref(self.grid), precision)
+            self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         self.seq = None
         if sequence_buffers:
             self._alloc_sequence()
@@ -79,6 +87,11 @@ class DeviceCase:
         fn = getattr(self.lib, name)
         rc = fn(C.byref(self.grid), C.c_void_p(self.stream), *args)
         abi.check(self.lib, rc)
+
+    def _transport(self) -> None:
+        self._call("flame_transport", _p(self.Q[self.cur]), _p(self.rhoi[self.cur]),
+                   _p(self.T[self.cur]), C.byref(self.thermo), C.byref(self.transport),
+                   self.precision)
 
     def _alloc_sequence(self):
         c = self.case
@@ -136,11 +149,12 @@ class DeviceCase:
         """The same stage as one flame_rk_stage launch (ping-pong of Q and rho_i)."""
         i, o = self.cur, 1 - self.cur
         b = FlameStageBuffers(_p(self.U), _p(self.Un), _p(self.Q[i]), _p(self.Q[o]),
-                              _p(self.rhoi[i]), _p(self.rhoi[o]), _p(self.rhon))
-        rc = self.lib.flame_rk_stage(C.byref(self.grid), C.c_void_p(self.stream), stage,
-                                     self.dt, C.byref(b), C.byref(self.cmetrics),
-                                     C.byref(self.thermo), C.byref(self.transport),
-                                     self.precision)
+                              _p(self.rhoi[i]), _p(self.rhoi[o]), _p(self.rhon),
+                              _p(self.T[i]), _p(self.T[o]), _p(self.scratch))
+        rc = self.lib.flame_rk_stage_tiled(C.byref(self.grid), C.c_void_p(self.stream), stage,
+                                           self.dt, C.byref(b), C.byref(self.cmetrics),
+                                           C.byref(self.thermo), C.byref(self.transport),
+                                           self.precision, self.tile)
         abi.check(self.lib, rc)
         self.cur = o
 
@@ -160,6 +174,7 @@ class DeviceCase:
         Q.copy_(Q_host, non_blocking=True)
         r.copy_(rhoi_host, non_blocking=True)
         self._call("flame_prim2c", _p(self.U), _p(Q))
+        self._transport()
         for _ in range(nsteps):
             self.step()
         Q_out.copy_(self.Q[self.cur], non_blocking=True)

@@ -184,25 +184,53 @@ int flame_specAdvance(const FlameGrid *g, flame_stream_t stream, double *rhoi, c
 
 /* ---------------------------------------------------------------------------------------
  * Fused path: one launch per RK3 stage (solver.jl:297-326 for periodic grids, IBM off).
- * Reads Q_in / rhoi_in (ghosts filled), writes U in place, Q_out / rhoi_out including their
- * periodic ghost images, so the caller swaps the in/out pair after every stage.
- * Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
+ * Reads Q_in / rhoi_in / trans_in (ghosts filled), writes U in place and Q_out / rhoi_out /
+ * trans_out including their periodic ghost images, so the caller swaps every in/out pair after
+ * each stage.  Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
+ * trans_* hold the transport of the state, (…, 3) = μ, λ, D, as computed by flame_transport;
+ * the stage computes the next one in its epilogue, so the law is evaluated once per cell.
+ * Q_* and trans_* are double arrays for precision 0 and float arrays for precision 1.
  * ------------------------------------------------------------------------------------- */
 typedef struct FlameStageBuffers {
     double *U;             /* (…,5) conserved, interior updated in place */
     double *Un;            /* (…,5) RK3 stage-0 copy */
-    const double *Q_in;    /* (…,7) primitives of the stage input, ghosts filled */
-    double *Q_out;         /* (…,7) primitives of the stage result, ghosts filled */
+    const void *Q_in;      /* (…,7) primitives of the stage input, ghosts filled */
+    void *Q_out;           /* (…,7) primitives of the stage result, ghosts filled */
     const double *rhoi_in; /* (…,ns) partial densities of the stage input, ghosts filled */
     double *rhoi_out;      /* (…,ns) partial densities of the stage result, ghosts filled */
     double *rhon;          /* (…,ns) RK3 stage-0 copy */
+    const void *trans_in;  /* (…,3) μ, λ, D of the stage input */
+    void *trans_out;       /* (…,3) μ, λ, D of the stage result */
+    void *scratch;         /* flame_stage_scratch_bytes() bytes for tile configuration 3, else
+                              unused (may be NULL); contents need not survive between calls */
 } FlameStageBuffers;
 
-/* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 split/recon/viscous,
- * FP64 accumulation, metrics and Newton temperature). */
+/* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 storage of Q and transport, FP32
+ * split / reconstruction / viscous fluxes; FP64 conserved accumulation, metrics, WENO-Z weights
+ * and Newton temperature).  No reference counterpart: it replaces the launch sequence of
+ * solver.jl:298-326. */
 int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                    const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *thermo,
                    const FlameTransport *transport, int precision);
+
+/* flame_rk_stage with an explicit configuration: 0, 1, 2 = one tile kernel per stage (16x8x8
+ * with one CTA per SM, 16x8x8 with two, 8x8x8 with two); 3 = four barrier-free launches
+ * (a prep pass and z, y, x warp-per-pencil sweeps) that need b->scratch.  The autotuner picks
+ * the configuration per grid, species count and precision. */
+int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
+                         const FlameStageBuffers *b, const FlameMetrics *m,
+                         const FlameThermo *thermo, const FlameTransport *transport,
+                         int precision, int tile);
+
+/* Bytes of scratch the pencil configuration needs: (5 + ns) doubles and (1 + ns) values of the
+ * storage type per ghosted point. */
+size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision);
+
+/* μ, λ, D of every ghosted point of a state (Q, rhoi) into trans (…, 3): the transport law of
+ * flame_mixture without the mass-fraction output; starts the fused stage loop. */
+int flame_transport(const FlameGrid *g, flame_stream_t stream, const void *Q, const double *rhoi,
+                    void *trans, const FlameThermo *thermo, const FlameTransport *transport,
+                    int precision);
 
 /* Message of the last error on the calling thread; returns its length. */
 int flame_last_error(char *buf, size_t n);

@@ -13,9 +13,22 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+_KEEP: list = []
+
+
 def _t(a):
+    """Device copy of a host array.  The tensor is kept alive until the next test so its
+    memory cannot be recycled by the caching allocator while a launch still reads it."""
     import torch
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release():
+    yield
+    _KEEP.clear()
 
 
 def _np(t):
