@@ -205,6 +205,71 @@ __device__ __forceinline__ T wenoz_minus(T V1, T V2, T V3, T V4, T V5) {
                             2 * V3 + 5 * V2 - V1);
 }
 
+// The same WENO-Z combination with one division instead of four: with b_k = ε + β_k,
+// α_k = d_k (1 + τ²/b_k²) and ω_k = α_k / Σα; multiplying every α_k by b_1² b_2² b_3² gives
+// A_k = d_k (b_k² + τ²) Π_{j≠k} b_j² with the same ratios.  Exact in real arithmetic; in FP64 it
+// differs from the reference's rounding by a few ulp (the products stay in range for |β| < 1e50).
+template <typename T>
+__device__ __forceinline__ T wenoz_combine_fast(T s11_, T s22_, T s33_, T v1, T v2, T v3) {
+    const double b1 = kWenoEps + double(s11_), b2 = kWenoEps + double(s22_),
+                 b3 = kWenoEps + double(s33_);
+    const double tau = fabs(double(s11_) - double(s33_));
+    const double t = tau * tau;
+    const double p1 = b1 * b1, p2 = b2 * b2, p3 = b3 * b3;
+    const double a1 = (p1 + t) * (p2 * p3);
+    const double a2 = 6.0 * (p2 + t) * (p1 * p3);
+    const double a3 = 3.0 * (p3 + t) * (p1 * p2);
+    return T((a1 * double(v1) + a2 * double(v2) + a3 * double(v3)) / (6.0 * (a1 + a2 + a3)));
+}
+
+template <typename T>
+__device__ __forceinline__ T wenoz_plus_fast(T V1, T V2, T V3, T V4, T V5) {
+    const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);
+    T a, b;
+    a = V1 - 2 * V2 + V3, b = V1 - 4 * V2 + 3 * V3;
+    const T s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V2 - V4;
+    const T s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V4 + V5, b = 3 * V3 - 4 * V4 + V5;
+    const T s33 = tmp1 * (a * a) + q4 * (b * b);
+    return wenoz_combine_fast<T>(s11, s22, s33, 2 * V1 - 7 * V2 + 11 * V3, -V2 + 5 * V3 + 2 * V4,
+                                 2 * V3 + 5 * V4 - V5);
+}
+
+template <typename T>
+__device__ __forceinline__ T wenoz_minus_fast(T V1, T V2, T V3, T V4, T V5) {
+    const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);
+    T a, b;
+    a = V5 - 2 * V4 + V3, b = V5 - 4 * V4 + 3 * V3;
+    const T s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V4 - V2;
+    const T s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V2 + V1, b = 3 * V3 - 4 * V2 + V1;
+    const T s33 = tmp1 * (a * a) + q4 * (b * b);
+    return wenoz_combine_fast<T>(s11, s22, s33, 11 * V3 - 7 * V4 + 2 * V5, -V4 + 5 * V3 + 2 * V2,
+                                 2 * V3 + 5 * V2 - V1);
+}
+
+// One face of the hybrid scheme for the fused paths: hybrid_face7 (below) with the
+// one-division WENO-Z weights.
+template <typename T>
+__device__ __forceinline__ T hybrid_face_fast(const T *p, const T *m, T phif) {
+    T fp, fm;
+    if (phif < T(kHybrid1)) {
+        fp = T(kUP7_2) * p[0] + T(kUP7_3) * p[1] + T(kUP7_4) * p[2] + T(kUP7_5) * p[3] +
+             T(kUP7_6) * p[4] + T(kUP7_7) * p[5];
+        fm = T(kUP7_7) * m[0] + T(kUP7_6) * m[1] + T(kUP7_5) * m[2] + T(kUP7_4) * m[3] +
+             T(kUP7_3) * m[4] + T(kUP7_2) * m[5];
+    } else if (phif < T(kHybrid2)) {
+        fp = wenoz_plus_fast(p[0], p[1], p[2], p[3], p[4]);
+        fm = wenoz_minus_fast(m[1], m[2], m[3], m[4], m[5]);
+    } else {
+        fp = p[2] + T(0.5) * minmod(p[3] - p[2], p[2] - p[1]);
+        fm = m[3] - T(0.5) * minmod(m[4] - m[3], m[3] - m[2]);
+    }
+    return fp + fm;
+}
+
 // One face of the hybrid scheme, schemes.jl:110-199.  p[0..6] = F+[c-3..c+3] (F+[c-4] has
 // weight UP7[1] = 0 and is not read), m[0..6] = F-[c-3..c+3]; the face lies between c-1 and c.
 template <typename T>

@@ -410,7 +410,7 @@ struct Tile {
                         mv[i] = sF[vm * L::NPMAX + p0 + i];
                     }
                     pv[6] = mv[6] = CT(0);
-                    G[n] = hybrid_face7<CT>(pv, mv, phif);
+                    G[n] = hybrid_face_fast<CT>(pv, mv, phif);
                 }
                 viscous_face<DIR>(gidx_face<DIR>(x, y, z), x, y, z, G);
 #pragma unroll

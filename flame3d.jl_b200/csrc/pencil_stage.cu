@@ -141,237 +141,189 @@ __device__ __forceinline__ void transport_point(const FlameThermo &th, const Fla
     D = lam / (rho * cpm);
 }
 
-// PASS: 0 = first sweep (writes R), 1 = middle (adds to R), 2 = last (finishes the stage).
-template <int DIR, int PASS, int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Wpb<DIR>::value * 32) k_pencil(const __grid_constant__ Args<QT> A) {
-    constexpr int WPB = Wpb<DIR>::value;
+// ---- phase A: everything the faces of a pencil need from one point, into the point's
+// column of shared memory (slot stride 32).  l is the point's position along the pencil.
+template <int DIR, int NS, typename QT, typename CT>
+__device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int g) {
     using SL = Slots<NS>;
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    CT *S = reinterpret_cast<CT *>(smem_raw) + warp * SL::N * 32;
-#define SV(slot, l) S[(slot) * 32 + (l)]
-
-    // ---- which pencil: warps of a block take consecutive cross-x positions for y/z sweeps
-    const int n_along = DIR == 0 ? A.nx : (DIR == 1 ? A.ny : A.nz);
-    const int nseg = (n_along + OWN - 1) / OWN;
-    const int gw = blockIdx.x * WPB + warp;
-    int seg, c1, c2;  // c1, c2: interior cross coordinates
-    if (DIR == 0) {
-        seg = gw % nseg;
-        const int r = gw / nseg;
-        c1 = r % A.ny, c2 = r / A.ny;  // y, z
-        if (c2 >= A.nz) return;
-    } else {
-        c1 = gw % A.nx;  // x
-        const int r = gw / A.nx;
-        seg = r % nseg;
-        c2 = r / nseg;  // z for DIR 1, y for DIR 2
-        if (c2 >= (DIR == 1 ? A.nz : A.ny)) return;
-    }
-    const int a = seg * OWN - 3 + lane;                    // interior along-coordinate
-    const int ga = clampi(a + A.ng, 0, n_along + 2 * A.ng - 1);  // ghosted, kept in the array
-    int gx, gy, gz;
-    if (DIR == 0) gx = ga, gy = c1 + A.ng, gz = c2 + A.ng;
-    else if (DIR == 1) gx = c1 + A.ng, gy = ga, gz = c2 + A.ng;
-    else gx = c1 + A.ng, gy = c2 + A.ng, gz = ga;
-    const int g = gx + A.sy * gy + A.sz * gz;
     const int np = A.np;
     const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
     const int s2 = D2 == 0 ? 1 : (D2 == 1 ? A.sy : A.sz);
     const QT *Q = A.Qi;
     const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
-
-    // ---- phase A: this lane's point
+#define SV(slot) S[(slot) * 32 + l]
+    const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]),
+             p = CT(Q[g + 4 * np]), T = CT(Q[g + 5 * np]), ei = CT(Q[g + 6 * np]);
+    const CT A1 = ldg<CT>(A.met[3 * DIR], g), A2 = ldg<CT>(A.met[3 * DIR + 1], g),
+             A3 = ldg<CT>(A.met[3 * DIR + 2], g);
+    // Steger-Warming split, split.jl:17-89 (divisions folded into reciprocals)
     {
-        const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]),
-                 p = CT(Q[g + 4 * np]), T = CT(Q[g + 5 * np]), ei = CT(Q[g + 6 * np]);
-        CT A1 = ldg<CT>(A.met[3 * DIR], g), A2 = ldg<CT>(A.met[3 * DIR + 1], g),
-           A3 = ldg<CT>(A.met[3 * DIR + 2], g);
-        // Steger-Warming split, split.jl:17-89 (divisions folded into reciprocals)
-        {
-            const CT gam = p * (CT(1) / ei) + 1;
-            const CT gm1 = gam - 1;
-            const CT inv = CT(1) / (rho * gam * gm1);
-            const CT cs = sqrt(gam * p * (gam * gm1 * inv));
-            const CT r2 = A1 * A1 + A2 * A2 + A3 * A3;
-            const CT rs = rsqrt(r2);
-            const CT ss = r2 * rs;
-            const CT E1 = A1 * u + A2 * v + A3 * w;
-            const CT E2 = E1 - cs * ss, E3 = E1 + cs * ss;
-            const CT B1 = A1 * rs, B2 = A2 * rs, B3 = A3 * rs;
-            const CT E1P = (E1 + fabs(E1)) * h, E2P = (E2 + fabs(E2)) * h, E3P = (E3 + fabs(E3)) * h;
-            const CT E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
-            const CT uc1 = u - cs * B1, uc2 = u + cs * B1;
-            const CT vc1 = v - cs * B2, vc2 = v + cs * B2;
-            const CT wc1 = w - cs * B3, wc2 = w + cs * B3;
-            const CT vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * h;
-            const CT vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * h;
-            const CT vv = gm1 * (u * u + v * v + w * w);
-            const CT W2 = (3 - gam) * (h * rho * gam * inv) * (cs * cs);
-            const CT tmp1 = h * rho * (rho * gm1 * inv);
-            const CT tmp2 = 2 * gm1;
-            SV(0, lane) = tmp1 * (tmp2 * E1P + E2P + E3P);
-            SV(1, lane) = tmp1 * (tmp2 * E1P * u + E2P * uc1 + E3P * uc2);
-            SV(2, lane) = tmp1 * (tmp2 * E1P * v + E2P * vc1 + E3P * vc2);
-            SV(3, lane) = tmp1 * (tmp2 * E1P * w + E2P * wc1 + E3P * wc2);
-            SV(4, lane) = tmp1 * (E1P * vv + E2P * vvc1 + E3P * vvc2 + W2 * (E2P + E3P));
-            SV(5, lane) = tmp1 * (tmp2 * E1M + E2M + E3M);
-            SV(6, lane) = tmp1 * (tmp2 * E1M * u + E2M * uc1 + E3M * uc2);
-            SV(7, lane) = tmp1 * (tmp2 * E1M * v + E2M * vc1 + E3M * vc2);
-            SV(8, lane) = tmp1 * (tmp2 * E1M * w + E2M * wc1 + E3M * wc2);
-            SV(9, lane) = tmp1 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
-            // species, split.jl:101-130
-            const CT Ep = h * (E1 + fabs(E1)), Em = h * (E1 - fabs(E1));
-#pragma unroll
-            for (int n = 0; n < NS; ++n) {
-                const CT r = CT(A.ri[g + n * np]);
-                SV(10 + n, lane) = Ep * r;
-                SV(10 + NS + n, lane) = Em * r;
-            }
-        }
-        SV(SL::Q4 + 0, lane) = u, SV(SL::Q4 + 1, lane) = v, SV(SL::Q4 + 2, lane) = w;
-        SV(SL::Q4 + 3, lane) = T;
-#pragma unroll
-        for (int m = 0; m < 10; ++m) SV(SL::MET + m, lane) = ldg<CT>(A.met[m], g);
-#pragma unroll
-        for (int m = 0; m < 3; ++m) SV(SL::TR + m, lane) = CT(A.Ti[g + m * np]);
-        SV(SL::RHO, lane) = rho;
-        SV(SL::PHI, lane) = CT(A.aux[g]);
+        const CT gam = p * (CT(1) / ei) + 1;
+        const CT gm1 = gam - 1;
+        const CT inv = CT(1) / (rho * gam * gm1);
+        const CT cs = sqrt(gam * p * (gam * gm1 * inv));
+        const CT r2 = A1 * A1 + A2 * A2 + A3 * A3;
+        const CT rs = rsqrt(r2);
+        const CT ss = r2 * rs;
+        const CT E1 = A1 * u + A2 * v + A3 * w;
+        const CT E2 = E1 - cs * ss, E3 = E1 + cs * ss;
+        const CT B1 = A1 * rs, B2 = A2 * rs, B3 = A3 * rs;
+        const CT E1P = (E1 + fabs(E1)) * h, E2P = (E2 + fabs(E2)) * h, E3P = (E3 + fabs(E3)) * h;
+        const CT E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
+        const CT uc1 = u - cs * B1, uc2 = u + cs * B1;
+        const CT vc1 = v - cs * B2, vc2 = v + cs * B2;
+        const CT wc1 = w - cs * B3, wc2 = w + cs * B3;
+        const CT vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * h;
+        const CT vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * h;
+        const CT vv = gm1 * (u * u + v * v + w * w);
+        const CT W2 = (3 - gam) * (h * rho * gam * inv) * (cs * cs);
+        const CT tmp1 = h * rho * (rho * gm1 * inv);
+        const CT tmp2 = 2 * gm1;
+        SV(0) = tmp1 * (tmp2 * E1P + E2P + E3P);
+        SV(1) = tmp1 * (tmp2 * E1P * u + E2P * uc1 + E3P * uc2);
+        SV(2) = tmp1 * (tmp2 * E1P * v + E2P * vc1 + E3P * vc2);
+        SV(3) = tmp1 * (tmp2 * E1P * w + E2P * wc1 + E3P * wc2);
+        SV(4) = tmp1 * (E1P * vv + E2P * vvc1 + E3P * vvc2 + W2 * (E2P + E3P));
+        SV(5) = tmp1 * (tmp2 * E1M + E2M + E3M);
+        SV(6) = tmp1 * (tmp2 * E1M * u + E2M * uc1 + E3M * uc2);
+        SV(7) = tmp1 * (tmp2 * E1M * v + E2M * vc1 + E3M * vc2);
+        SV(8) = tmp1 * (tmp2 * E1M * w + E2M * wc1 + E3M * wc2);
+        SV(9) = tmp1 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
+        // species, split.jl:101-130
+        const CT Ep = h * (E1 + fabs(E1)), Em = h * (E1 - fabs(E1));
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-            const QT *Y = A.aux + (1 + n) * np;
-            SV(SL::Y + n, lane) = CT(Y[g]);
-            SV(SL::DY1 + n, lane) = CT(Y[g + s1]) - CT(Y[g - s1]);
-            SV(SL::DY2 + n, lane) = CT(Y[g + s2]) - CT(Y[g - s2]);
-        }
-        // cell-centred 4th-order tangential derivatives of u, v, w, T; the face value the
-        // reference forms (viscous.jl:36-53) is the mean of the two cells' values
-        const int qv[4] = {1, 2, 3, 5};
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const QT *q = Q + qv[m] * np + g;
-            SV(SL::DQ1 + m, lane) = c23 * (CT(q[s1]) - CT(q[-s1])) - c12 * (CT(q[2 * s1]) - CT(q[-2 * s1]));
-            SV(SL::DQ2 + m, lane) = c23 * (CT(q[s2]) - CT(q[-s2])) - c12 * (CT(q[2 * s2]) - CT(q[-2 * s2]));
+            const CT r = CT(A.ri[g + n * np]);
+            SV(10 + n) = Ep * r;
+            SV(10 + NS + n) = Em * r;
         }
     }
-    __syncwarp();
-
-    // ---- phase B: face between lanes l-1 and l (faces of the owned cells and one more)
-    CT G[5 + NS];
-    const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
-    if (face) {
-        const int l = lane, lm = lane - 1;
-        const CT phif = CT(jmax(double(SV(SL::PHI, lm)), double(SV(SL::PHI, l))));
+    SV(SL::Q4 + 0) = u, SV(SL::Q4 + 1) = v, SV(SL::Q4 + 2) = w, SV(SL::Q4 + 3) = T;
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) {
-            const int vp = n < 5 ? n : 5 + n;
-            const int vm = n < 5 ? 5 + n : 5 + NS + n;
-            CT pv[7], mv[7];
+    for (int m = 0; m < 10; ++m) SV(SL::MET + m) = ldg<CT>(A.met[m], g);
 #pragma unroll
-            for (int i = 0; i < 6; ++i) pv[i] = SV(vp, l - 3 + i), mv[i] = SV(vm, l - 3 + i);
-            pv[6] = mv[6] = CT(0);
-            G[n] = hybrid_face7<CT>(pv, mv, phif);
-        }
-        CT met[9];
+    for (int m = 0; m < 3; ++m) SV(SL::TR + m) = CT(A.Ti[g + m * np]);
+    SV(SL::RHO) = rho;
+    SV(SL::PHI) = CT(A.aux[g]);
 #pragma unroll
-        for (int m = 0; m < 9; ++m) met[m] = (SV(SL::MET + m, lm) + SV(SL::MET + m, l)) * h;
-        const CT Jac = (SV(SL::MET + 9, lm) + SV(SL::MET + 9, l)) * h;
-        const CT mui = (SV(SL::TR, lm) + SV(SL::TR, l)) * h;
-        const CT lami = (SV(SL::TR + 1, lm) + SV(SL::TR + 1, l)) * h;
-        const CT DL = SV(SL::TR + 2, lm), DR = SV(SL::TR + 2, l);
-        const CT rho = (SV(SL::RHO, lm) + SV(SL::RHO, l)) * h;
-        const CT Tf = (SV(SL::Q4 + 3, lm) + SV(SL::Q4 + 3, l)) * h;
-        const CT *md = met + 3 * DIR;
-        // species diffusion (viscous.jl:430-507) first: it yields Fh for the energy flux
-        CT Vk1[NS], Vk2[NS], Vk3[NS], Yf[NS];
-        CT sum1 = 0, sum2 = 0, sum3 = 0;
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-            const CT y0 = SV(SL::Y + n, l), ym = SV(SL::Y + n, lm);
-            const CT yp = SV(SL::Y + n, l + 1), ymm = SV(SL::Y + n, l - 2);
-            CT dY[3];
-            dY[DIR] = CT(1.25) * (y0 - ym) - c12 * (yp - ymm);
-            dY[D1] = CT(0.25) * (SV(SL::DY1 + n, l) + SV(SL::DY1 + n, lm));
-            dY[D2] = CT(0.25) * (SV(SL::DY2 + n, l) + SV(SL::DY2 + n, lm));
-            const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
-            const CT Vx = (dY[0] * met[0] + dY[1] * met[3] + dY[2] * met[6]) * Jac * rhoDi;
-            const CT Vy = (dY[0] * met[1] + dY[1] * met[4] + dY[2] * met[7]) * Jac * rhoDi;
-            const CT Vz = (dY[0] * met[2] + dY[1] * met[5] + dY[2] * met[8]) * Jac * rhoDi;
-            Vk1[n] = Vx, Vk2[n] = Vy, Vk3[n] = Vz;
-            sum1 += Vx, sum2 += Vy, sum3 += Vz;
-            Yf[n] = h * (ym + y0);
-        }
-        CT fh1 = 0, fh2 = 0, fh3 = 0;
-        {
-            const double Td = double(Tf);
-            const double T2 = 0.5 * Td * Td, T3 = 2.0 / 3.0 * T2 * Td, T4 = T2 * T2,
-                         T5 = 0.8 * T4 * Td;
-#pragma unroll
-            for (int n = 0; n < NS; ++n) {
-                const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
-                const CT V1 = Vk1[n] - sum1 * Yf[n], V2 = Vk2[n] - sum2 * Yf[n],
-                         V3 = Vk3[n] - sum3 * Yf[n];
-                G[5 + n] -= V1 * md[0] + V2 * md[1] + V3 * md[2];
-                fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
-            }
-        }
-        // momentum and energy, viscous.jl:14-141
-        CT gr[4][3];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            CT dq[3];
-            dq[DIR] = CT(1.25) * (SV(SL::Q4 + m, l) - SV(SL::Q4 + m, lm)) -
-                      c12 * (SV(SL::Q4 + m, l + 1) - SV(SL::Q4 + m, l - 2));
-            dq[D1] = h * (SV(SL::DQ1 + m, l) + SV(SL::DQ1 + m, lm));
-            dq[D2] = h * (SV(SL::DQ2 + m, l) + SV(SL::DQ2 + m, lm));
-#pragma unroll
-            for (int x = 0; x < 3; ++x)
-                gr[m][x] = (dq[0] * met[x] + dq[1] * met[3 + x] + dq[2] * met[6 + x]) * Jac;
-        }
-        const CT u = (SV(SL::Q4 + 0, lm) + SV(SL::Q4 + 0, l)) * h;
-        const CT v = (SV(SL::Q4 + 1, lm) + SV(SL::Q4 + 1, l)) * h;
-        const CT w = (SV(SL::Q4 + 2, lm) + SV(SL::Q4 + 2, l)) * h;
-        const CT div = gr[0][0] + gr[1][1] + gr[2][2];
-        const CT t11 = mui * (2 * gr[0][0] - c23 * div);
-        const CT t12 = mui * (gr[0][1] + gr[1][0]);
-        const CT t13 = mui * (gr[0][2] + gr[2][0]);
-        const CT t22 = mui * (2 * gr[1][1] - c23 * div);
-        const CT t23 = mui * (gr[2][1] + gr[1][2]);
-        const CT t33 = mui * (2 * gr[2][2] - c23 * div);
-        const CT E1 = u * t11 + v * t12 + w * t13 + lami * gr[3][0] + fh1;
-        const CT E2 = u * t12 + v * t22 + w * t23 + lami * gr[3][1] + fh2;
-        const CT E3 = u * t13 + v * t23 + w * t33 + lami * gr[3][2] + fh3;
-        G[1] -= md[0] * t11 + md[1] * t12 + md[2] * t13;
-        G[2] -= md[0] * t12 + md[1] * t22 + md[2] * t23;
-        G[3] -= md[0] * t13 + md[1] * t23 + md[2] * t33;
-        G[4] -= md[0] * E1 + md[1] * E2 + md[2] * E3;
+    for (int n = 0; n < NS; ++n) {
+        const QT *Y = A.aux + (1 + n) * np;
+        SV(SL::Y + n) = CT(Y[g]);
+        SV(SL::DY1 + n) = CT(Y[g + s1]) - CT(Y[g - s1]);
+        SV(SL::DY2 + n) = CT(Y[g + s2]) - CT(Y[g - s2]);
     }
-    __syncwarp();
-    if (face) {
+    // cell-centred 4th-order tangential derivatives of u, v, w, T; the face value the reference
+    // forms (viscous.jl:36-53) is the mean of the two cells' values
+    const int qv[4] = {1, 2, 3, 5};
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) SV(SL::G + n, lane) = G[n];
+    for (int m = 0; m < 4; ++m) {
+        const QT *q = Q + qv[m] * np + g;
+        SV(SL::DQ1 + m) = c23 * (CT(q[s1]) - CT(q[-s1])) - c12 * (CT(q[2 * s1]) - CT(q[-2 * s1]));
+        SV(SL::DQ2 + m) = c23 * (CT(q[s2]) - CT(q[-s2])) - c12 * (CT(q[2 * s2]) - CT(q[-2 * s2]));
     }
-    __syncwarp();
-
-    // ---- phase C: the owned cell of this lane
-    if (lane < 3 || lane >= 3 + OWN || a >= n_along) return;
-    double rhs[5 + NS];
-#pragma unroll
-    for (int n = 0; n < 5 + NS; ++n)
-        rhs[n] = double(SV(SL::G + n, lane)) - double(SV(SL::G + n, lane + 1));
 #undef SV
-    if (PASS == 0) {
+}
+
+// ---- phase B: the face between pencil positions l-1 and l; G = F_inviscid − F_viscous.
+template <int DIR, int NS, typename QT, typename CT>
+__device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G) {
+    using SL = Slots<NS>;
+    constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
+    const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
+#define SV(slot, ll) S[(slot) * 32 + (ll)]
+    const int lm = l - 1;
+    const CT phif = CT(jmax(double(SV(SL::PHI, lm)), double(SV(SL::PHI, l))));
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * np] = rhs[n];
-        return;
-    }
-    if (PASS == 1) {
+    for (int n = 0; n < 5 + NS; ++n) {
+        const int vp = n < 5 ? n : 5 + n;
+        const int vm = n < 5 ? 5 + n : 5 + NS + n;
+        CT pv[7], mv[7];
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * np] += rhs[n];
-        return;
+        for (int i = 0; i < 6; ++i) pv[i] = SV(vp, l - 3 + i), mv[i] = SV(vm, l - 3 + i);
+        pv[6] = mv[6] = CT(0);
+        G[n] = hybrid_face_fast<CT>(pv, mv, phif);
     }
-    // last sweep: div, RK3 combination, c2Prim, transport, ghost images
+    CT met[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) met[m] = (SV(SL::MET + m, lm) + SV(SL::MET + m, l)) * h;
+    const CT Jac = (SV(SL::MET + 9, lm) + SV(SL::MET + 9, l)) * h;
+    const CT mui = (SV(SL::TR, lm) + SV(SL::TR, l)) * h;
+    const CT lami = (SV(SL::TR + 1, lm) + SV(SL::TR + 1, l)) * h;
+    const CT DL = SV(SL::TR + 2, lm), DR = SV(SL::TR + 2, l);
+    const CT rho = (SV(SL::RHO, lm) + SV(SL::RHO, l)) * h;
+    const CT Tf = (SV(SL::Q4 + 3, lm) + SV(SL::Q4 + 3, l)) * h;
+    const CT *md = met + 3 * DIR;
+    // species diffusion (viscous.jl:430-507) first: it yields Fh for the energy flux
+    CT Vk1[NS], Vk2[NS], Vk3[NS], Yf[NS];
+    CT sum1 = 0, sum2 = 0, sum3 = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        const CT y0 = SV(SL::Y + n, l), ym = SV(SL::Y + n, lm);
+        const CT yp = SV(SL::Y + n, l + 1), ymm = SV(SL::Y + n, l - 2);
+        CT dY[3];
+        dY[DIR] = CT(1.25) * (y0 - ym) - c12 * (yp - ymm);
+        dY[D1] = CT(0.25) * (SV(SL::DY1 + n, l) + SV(SL::DY1 + n, lm));
+        dY[D2] = CT(0.25) * (SV(SL::DY2 + n, l) + SV(SL::DY2 + n, lm));
+        const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
+        const CT Vx = (dY[0] * met[0] + dY[1] * met[3] + dY[2] * met[6]) * Jac * rhoDi;
+        const CT Vy = (dY[0] * met[1] + dY[1] * met[4] + dY[2] * met[7]) * Jac * rhoDi;
+        const CT Vz = (dY[0] * met[2] + dY[1] * met[5] + dY[2] * met[8]) * Jac * rhoDi;
+        Vk1[n] = Vx, Vk2[n] = Vy, Vk3[n] = Vz;
+        sum1 += Vx, sum2 += Vy, sum3 += Vz;
+        Yf[n] = h * (ym + y0);
+    }
+    CT fh1 = 0, fh2 = 0, fh3 = 0;
+    {
+        const double Td = double(Tf);
+        const double T2 = 0.5 * Td * Td, T3 = 2.0 / 3.0 * T2 * Td, T4 = T2 * T2, T5 = 0.8 * T4 * Td;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
+            const CT V1 = Vk1[n] - sum1 * Yf[n], V2 = Vk2[n] - sum2 * Yf[n],
+                     V3 = Vk3[n] - sum3 * Yf[n];
+            G[5 + n] -= V1 * md[0] + V2 * md[1] + V3 * md[2];
+            fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
+        }
+    }
+    // momentum and energy, viscous.jl:14-141
+    CT gr[4][3];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        CT dq[3];
+        dq[DIR] = CT(1.25) * (SV(SL::Q4 + m, l) - SV(SL::Q4 + m, lm)) -
+                  c12 * (SV(SL::Q4 + m, l + 1) - SV(SL::Q4 + m, l - 2));
+        dq[D1] = h * (SV(SL::DQ1 + m, l) + SV(SL::DQ1 + m, lm));
+        dq[D2] = h * (SV(SL::DQ2 + m, l) + SV(SL::DQ2 + m, lm));
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            gr[m][x] = (dq[0] * met[x] + dq[1] * met[3 + x] + dq[2] * met[6 + x]) * Jac;
+    }
+    const CT u = (SV(SL::Q4 + 0, lm) + SV(SL::Q4 + 0, l)) * h;
+    const CT v = (SV(SL::Q4 + 1, lm) + SV(SL::Q4 + 1, l)) * h;
+    const CT w = (SV(SL::Q4 + 2, lm) + SV(SL::Q4 + 2, l)) * h;
+#undef SV
+    const CT div = gr[0][0] + gr[1][1] + gr[2][2];
+    const CT t11 = mui * (2 * gr[0][0] - c23 * div);
+    const CT t12 = mui * (gr[0][1] + gr[1][0]);
+    const CT t13 = mui * (gr[0][2] + gr[2][0]);
+    const CT t22 = mui * (2 * gr[1][1] - c23 * div);
+    const CT t23 = mui * (gr[2][1] + gr[1][2]);
+    const CT t33 = mui * (2 * gr[2][2] - c23 * div);
+    const CT E1 = u * t11 + v * t12 + w * t13 + lami * gr[3][0] + fh1;
+    const CT E2 = u * t12 + v * t22 + w * t23 + lami * gr[3][1] + fh2;
+    const CT E3 = u * t13 + v * t23 + w * t33 + lami * gr[3][2] + fh3;
+    G[1] -= md[0] * t11 + md[1] * t12 + md[2] * t13;
+    G[2] -= md[0] * t12 + md[1] * t22 + md[2] * t23;
+    G[3] -= md[0] * t13 + md[1] * t23 + md[2] * t33;
+    G[4] -= md[0] * E1 + md[1] * E2 + md[2] * E3;
+}
+
+// ---- last sweep: div, RK3 combination, c2Prim, transport, ghost images of one cell.
+template <int NS, typename QT>
+__device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, int gy, int gz,
+                                            const double *rhs) {
+    const int np = A.np;
     const double Jact = A.met[9][g] * A.dt;
     double Uc[5], r[NS];
 #pragma unroll
@@ -391,6 +343,7 @@ __global__ void __launch_bounds__(Wpb<DIR>::value * 32) k_pencil(const __grid_co
         if (A.stage > 1) rv = rv * A.ca + A.rn[g + n * np] * A.cb;
         r[n] = rv;
     }
+    // c2Prim, utils.jl:2-48
     const double rho = jmax(Uc[0], kEps);
     const double rinv = 1 / rho;
     double sr = 0.0;
@@ -407,6 +360,8 @@ __global__ void __launch_bounds__(Wpb<DIR>::value * 32) k_pencil(const __grid_co
     transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
     const double qv[7] = {rho, u, v, w, p, Tn, ei};
     const double tv[3] = {mu, lam, D};
+    // the cell and its periodic ghost images (new: the reference fills ghosts with case-specific
+    // kernels, boundary.jl:1-191)
     const int ng = A.ng;
     int ox[2] = {0, 0}, oy[2] = {0, 0}, oz[2] = {0, 0};
     int nxo = 1, nyo = 1, nzo = 1;
@@ -424,6 +379,112 @@ __global__ void __launch_bounds__(Wpb<DIR>::value * 32) k_pencil(const __grid_co
 #pragma unroll
                 for (int n = 0; n < NS; ++n) A.ro[t + n * np] = r[n];
             }
+}
+
+// x sweep (lanes along x, every access coalesced); it is the last sweep and finishes the stage.
+template <int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_constant__ Args<QT> A) {
+    constexpr int WPB = Wpb<0>::value;
+    using SL = Slots<NS>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    CT *S = reinterpret_cast<CT *>(smem_raw) + warp * SL::N * 32;
+    const int nseg = (A.nx + OWN - 1) / OWN;
+    const int gw = blockIdx.x * WPB + warp;
+    const int seg = gw % nseg;
+    const int y = (gw / nseg) % A.ny, z = (gw / nseg) / A.ny;
+    if (z >= A.nz) return;
+    const int a = seg * OWN - 3 + lane;
+    const int gx = clampi(a + A.ng, 0, A.nx + 2 * A.ng - 1), gy = y + A.ng, gz = z + A.ng;
+    const int g = gx + A.sy * gy + A.sz * gz;
+    point_phase<0, NS, QT, CT>(A, S, lane, g);
+    __syncwarp();
+    CT G[5 + NS];
+    const bool face = lane >= 3 && lane <= 3 + OWN && a <= A.nx;
+    if (face) face_phase<0, NS, QT, CT>(A, S, lane, G);
+    __syncwarp();
+    if (face) {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) S[(SL::G + n) * 32 + lane] = G[n];
+    }
+    __syncwarp();
+    if (lane < 3 || lane >= 3 + OWN || a >= A.nx) return;
+    double rhs[5 + NS];
+#pragma unroll
+    for (int n = 0; n < 5 + NS; ++n)
+        rhs[n] = double(S[(SL::G + n) * 32 + lane]) - double(S[(SL::G + n) * 32 + lane + 1]);
+    finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
+}
+
+// Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
+// use whole 128-byte lines; 8 when the column slots would not fit in shared memory.
+template <int NS, typename CT>
+struct Staged {
+    static constexpr int COLS = (sizeof(CT) * Slots<NS>::N * 33 * 16 <= 200 * 1024) ? 16 : 8;
+    static constexpr int STRIDE = Slots<NS>::N * 32 + 1;  // padded column region (bank spread)
+};
+
+// y or z sweep (DIR 1, 2).  The block stages the points of COLS neighbouring pencils with
+// x-fastest threads (coalesced loads), then each warp works its own pencil from shared memory
+// exactly like the x sweep, and the right-hand side goes back with x-fastest threads.
+// PASS 0 writes R, PASS 1 adds to it.
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
+    k_pencil_staged(const __grid_constant__ Args<QT> A) {
+    constexpr int COLS = Staged<NS, CT>::COLS, STRIDE = Staged<NS, CT>::STRIDE;
+    using SL = Slots<NS>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT *base = reinterpret_cast<CT *>(smem_raw);
+    const int n_along = DIR == 1 ? A.ny : A.nz;
+    const int n_c2 = DIR == 1 ? A.nz : A.ny;
+    const int nseg = (n_along + OWN - 1) / OWN;
+    const int nxb = (A.nx + COLS - 1) / COLS;
+    int bid = blockIdx.x;
+    const int xb = bid % nxb;
+    bid /= nxb;
+    const int seg = bid % nseg, c2 = bid / nseg;
+    if (c2 >= n_c2) return;
+    const int tid = threadIdx.x;
+    // ---- phase A, x-fastest: thread -> (column cx, pencil position l)
+    {
+        const int cx = tid % COLS, l = tid / COLS;
+        const int x = clampi(xb * COLS + cx, 0, A.nx - 1);
+        const int a = seg * OWN - 3 + l;
+        const int ga = clampi(a + A.ng, 0, n_along + 2 * A.ng - 1);
+        const int gx = x + A.ng;
+        const int gy = DIR == 1 ? ga : c2 + A.ng;
+        const int gz = DIR == 1 ? c2 + A.ng : ga;
+        point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
+    }
+    __syncthreads();
+    // ---- phase B, one warp per pencil (column)
+    const int warp = tid >> 5, lane = tid & 31;
+    CT *S = base + warp * STRIDE;
+    const int a = seg * OWN - 3 + lane;
+    CT G[5 + NS];
+    const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
+    if (face) face_phase<DIR, NS, QT, CT>(A, S, lane, G);
+    __syncwarp();
+    if (face) {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) S[(SL::G + n) * 32 + lane] = G[n];
+    }
+    __syncthreads();
+    // ---- phase C, x-fastest again: cell differences into R
+    const int cx = tid % COLS, l = tid / COLS;
+    const int x = xb * COLS + cx;
+    const int ac = seg * OWN - 3 + l;
+    if (l < 3 || l >= 3 + OWN || ac >= n_along || x >= A.nx) return;
+    const int gy = DIR == 1 ? ac + A.ng : c2 + A.ng;
+    const int gz = DIR == 1 ? c2 + A.ng : ac + A.ng;
+    const int g = (x + A.ng) + A.sy * gy + A.sz * gz;
+    const CT *Sc = base + cx * STRIDE;
+#pragma unroll
+    for (int n = 0; n < 5 + NS; ++n) {
+        const double d = double(Sc[(SL::G + n) * 32 + l]) - double(Sc[(SL::G + n) * 32 + l + 1]);
+        if (PASS == 0) A.R[g + n * A.np] = d;
+        else A.R[g + n * A.np] += d;
+    }
 }
 
 template <typename QT>
@@ -455,28 +516,41 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
     return A;
 }
 
-template <int DIR, int PASS, int NS, typename QT, typename CT>
-int launch_sweep(const Args<QT> &A, cudaStream_t s) {
-    constexpr int WPB = Wpb<DIR>::value;
-    constexpr size_t sm = smem_bytes<NS, CT, WPB>();
-    static bool attr_set[64] = {};
+template <typename K>
+int set_smem(K kernel, size_t sm, bool *done) {
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_pencil<DIR, PASS, NS, QT, CT>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess)
-            return flame_fail(FLAME_ELAUNCH, "pencil sweep: %zu B shared memory: %s", sm,
-                              cudaGetErrorString(e));
-        if (dev >= 0 && dev < 64) attr_set[dev] = true;
-    }
-    const int n_along = DIR == 0 ? A.nx : (DIR == 1 ? A.ny : A.nz);
-    const int nseg = (n_along + OWN - 1) / OWN;
-    const long long cross = DIR == 0 ? (long long)A.ny * A.nz
-                                     : (long long)A.nx * (DIR == 1 ? A.nz : A.ny);
-    const long long warps = cross * nseg;
-    const unsigned blocks = (unsigned)((warps + WPB - 1) / WPB);
-    k_pencil<DIR, PASS, NS, QT, CT><<<blocks, WPB * 32, sm, s>>>(A);
+    if (dev >= 0 && dev < 64 && done[dev]) return FLAME_OK;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess)
+        return flame_fail(FLAME_ELAUNCH, "pencil sweep: %zu B shared memory: %s", sm,
+                          cudaGetErrorString(e));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return FLAME_OK;
+}
+
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+int launch_staged(const Args<QT> &A, cudaStream_t s) {
+    using ST = Staged<NS, CT>;
+    constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
+    static bool done[64] = {};
+    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT>, sm, done)) return e;
+    const int n_along = DIR == 1 ? A.ny : A.nz;
+    const int n_c2 = DIR == 1 ? A.nz : A.ny;
+    const long long blocks = (long long)((A.nx + ST::COLS - 1) / ST::COLS) *
+                             ((n_along + OWN - 1) / OWN) * n_c2;
+    k_pencil_staged<DIR, PASS, NS, QT, CT><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    return flame_check_launch("flame_rk_stage (pencil)");
+}
+
+template <int NS, typename QT, typename CT>
+int launch_x(const Args<QT> &A, cudaStream_t s) {
+    constexpr int WPB = Wpb<0>::value;
+    constexpr size_t sm = smem_bytes<NS, CT, WPB>();
+    static bool done[64] = {};
+    if (int e = set_smem(k_pencil_x<NS, QT, CT>, sm, done)) return e;
+    const long long warps = (long long)A.ny * A.nz * ((A.nx + OWN - 1) / OWN);
+    k_pencil_x<NS, QT, CT><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
@@ -487,9 +561,9 @@ int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const Flame
     const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr, scratch);
     k_prep<NS, QT><<<(unsigned)((A.np + 255) / 256), 256, 0, s>>>(A);
     if (int e = flame_check_launch("flame_rk_stage (prep)")) return e;
-    if (int e = launch_sweep<2, 0, NS, QT, CT>(A, s)) return e;
-    if (int e = launch_sweep<1, 1, NS, QT, CT>(A, s)) return e;
-    return launch_sweep<0, 2, NS, QT, CT>(A, s);
+    if (int e = launch_staged<2, 0, NS, QT, CT>(A, s)) return e;
+    if (int e = launch_staged<1, 1, NS, QT, CT>(A, s)) return e;
+    return launch_x<NS, QT, CT>(A, s);
 }
 
 template <typename QT, typename CT>

@@ -61,7 +61,7 @@ def test_argument_errors_need_no_gpu(f3d, lib):
     assert "ns=0" in f3d.abi.last_error(lib)
     # the fused stage refuses non-periodic grids and unknown precisions before launching
     g = f3d.FlameGrid(8, 8, 8, 4, 1, 3)
-    b = f3d.FlameStageBuffers(1, 2, 3, 4, 5, 6, 7)
+    b = f3d.FlameStageBuffers(1, 2, 3, 4, 5, 6, 7, 8, 9)
     m = f3d.FlameMetrics(*([1] * 10))
     th, tr = f3d.FlameThermo(), f3d.FlameTransport()
     rc = lib.flame_rk_stage(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m), C.byref(th),
@@ -71,7 +71,7 @@ def test_argument_errors_need_no_gpu(f3d, lib):
     rc = lib.flame_rk_stage(C.byref(g), None, 4, 1e-3, C.byref(b), C.byref(m), C.byref(th),
                             C.byref(tr), 0)
     assert rc == 1 and "stage" in f3d.abi.last_error(lib)
-    b2 = f3d.FlameStageBuffers(1, 2, 3, 3, 5, 6, 7)
+    b2 = f3d.FlameStageBuffers(1, 2, 3, 3, 5, 6, 7, 8, 9)
     rc = lib.flame_rk_stage(C.byref(g), None, 1, 1e-3, C.byref(b2), C.byref(m), C.byref(th),
                             C.byref(tr), 0)
     assert rc == 1 and "differ" in f3d.abi.last_error(lib)
