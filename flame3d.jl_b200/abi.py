@@ -93,6 +93,7 @@ SIGNATURES = {
     "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
     "flame_rk_stage_tiled": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I, I],
+    "flame_rk_stage_noalloc": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
     "flame_transport": [G, S, P, P, P, TH, TR, I],
     "flame_stage_scratch_bytes": [G, I],
     "flame_last_error": [C.c_char_p, C.c_size_t],

@@ -226,6 +226,23 @@ int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, d
  * storage type per ghosted point. */
 size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision);
 
+/* No counterpart in the reference.  The pencil-sweep stage (configuration 3) for callers that
+ * cannot allocate device memory for it: a Julia program whose device memory all belongs to
+ * CUDA.jl's pool, or a serving process that has committed its whole HBM budget, must not have
+ * the library cudaMalloc for them, and an allocation can synchronize the device.  The scratch
+ * lives in one array of FLAME_NOALLOC_SCRATCH_BYTES (64 MiB) that the library's GPU code holds
+ * on every device it is loaded on until the process exits; b->scratch is ignored.  Grids whose
+ * flame_stage_scratch_bytes() exceeds it are rejected with FLAME_EINVAL (FP64, ns = 1: up to
+ * about one million ghosted points).  The first call on a device looks up the array's address
+ * with that device current, so make it before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU race and must be serialised by the caller.  Nothing
+ * in the array has to start at zero; allocates nothing. */
+#define FLAME_NOALLOC_SCRATCH_BYTES (64u << 20)
+int flame_rk_stage_noalloc(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
+                           const FlameStageBuffers *b, const FlameMetrics *m,
+                           const FlameThermo *thermo, const FlameTransport *transport,
+                           int precision);
+
 /* μ, λ, D of every ghosted point of a state (Q, rhoi) into trans (…, 3): the transport law of
  * flame_mixture without the mass-fraction output; starts the fused stage loop. */
 int flame_transport(const FlameGrid *g, flame_stream_t stream, const void *Q, const double *rhoi,
