@@ -8,8 +8,10 @@ one-launch-per-stage kernel.  A "step" is one SSP-RK3 step (three stages).
          steps (max over ranks; N ranks run N independent replicas: weak scaling)
   e2e    the same metric through the public host-buffer call (DeviceCase.advance_from_host):
          every step uploads the ghosted Q and rho_i from pinned memory and downloads them
-  roofline  the fused stage kernel (the only kernel in the timed loop) against the measured
-         HBM copy bandwidth, with B_alg = 8 (41 + 3 Ns + [Ns >= 2] Ns) bytes per cell-stage
+  roofline  one RK3 stage (the unit the algorithmic bytes are defined for: one fused launch in
+         configurations 0-2, the prep pass and three pencil sweeps in configuration 3) against
+         the measured HBM copy bandwidth, with B_alg = 8 (41 + 3 Ns + [Ns >= 2] Ns) bytes per
+         interior cell-stage; `traffic` is the DRAM bytes per stage from an ncu capture
   cpu_baseline  the oracle (C++ FP64 restatement, OpenMP over all host cores) on a bounded
          sample of the same workload
 
@@ -197,7 +199,7 @@ def run_reference(args, f3d):
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="jet256x128x128", choices=sorted(WORKLOADS))
@@ -258,7 +260,7 @@ def main() -> int:
     stages = 3 * args.steps
     cells = case.cells
     value = world * cells * stages / (ms / 1e3) / 1e6
-    kernel_ms = ms / stages  # the fused stage kernel is the only launch in the loop
+    stage_ms = ms / stages  # device time of one stage (all of its launches)
 
     # ---- end to end through the host-buffer API (pinned host memory, copies timed)
     ns = case.ns
@@ -289,21 +291,21 @@ def main() -> int:
             dist.destroy_process_group()
         return 0
 
-    # ---- roofline of the fused stage kernel
+    # ---- roofline of one stage
     peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     balg = b_alg(ns, prec)
-    achieved = balg * cells / (kernel_ms / 1e3) / 1e9
+    achieved = balg * cells / (stage_ms / 1e3) / 1e9
     traffic = None
     if TRAFFIC.exists():
-        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}")
+        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}:{dc.tile}")
         if tr:
-            traffic = tr.get("bytes_per_launch")
+            traffic = tr.get("bytes_per_stage")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "peak_source": "measured" if PEAKS.exists() else "fallback",
-            "kernel": "flame::fused::k_stage", "b_alg_bytes_per_cell": balg,
-            "kernel_ms": kernel_ms}
+            "kernel": dc.stage_kernels(), "b_alg_bytes_per_cell": balg,
+            "stage_ms": stage_ms}
 
     cpu = None
     if not args.no_cpu:
@@ -318,14 +320,14 @@ def main() -> int:
            "dtype": "f64" if prec == 0 else "f32/f64",
            "data": "synthetic (seeded jet on the wavy periodic mapping)",
            "config": {"workload": args.workload, "cells": cells, "species": ns,
-                      "precision": args.precision, "path": "fused one launch per RK3 stage",
+                      "precision": args.precision, "path": dc.stage_kernels(), "stage_config": dc.tile,
                       "l2": "inputs larger than L2 (state ~%.1f GB per replica)" % (
                           (35 + 3 * ns) * case.Q[0].size * 8 / 1e9),
                       "parallelism": f"replicas x{world}"},
            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
-           "gpu_launches": stages}
+           "gpu_launches": stages * dc.launches_per_stage()}
     print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -158,6 +158,15 @@ class DeviceCase:
         abi.check(self.lib, rc)
         self.cur = o
 
+    def launches_per_stage(self) -> int:
+        """Kernels one fused stage launches: 4 for the pencil sweeps, 1 for a tile kernel."""
+        return 4 if self.tile == 3 else 1
+
+    def stage_kernels(self) -> str:
+        if self.tile == 3:
+            return "pencil::k_prep + k_pencil_staged<z> + k_pencil_staged<y> + k_pencil_x"
+        return "fused::k_stage<tile %d>" % self.tile
+
     def step(self, fused: bool = True) -> None:
         for s in (1, 2, 3):
             (self.stage_fused if fused else self.stage_sequence)(s)
