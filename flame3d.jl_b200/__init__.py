@@ -16,6 +16,12 @@ __all__ = ["FlameError", "FlameGrid", "FlameMetrics", "FlameStageBuffers", "Flam
            "ideal_air", "synthetic_species"]
 
 
+def batch_module():
+    """The batched-stage module (torch-backed, imported lazily)."""
+    import importlib
+    return importlib.import_module(__name__ + ".batch")
+
+
 def solver_module():
     """The torch-backed solver module (imported lazily so `import flame3d_b200` stays light)."""
     import importlib

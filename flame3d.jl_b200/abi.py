@@ -60,6 +60,12 @@ class FlameStageBuffers(C.Structure):
                                           "rhon", "trans_in", "trans_out", "scratch")]
 
 
+class FlameCaseDesc(C.Structure):
+    _fields_ = [("grid", FlameGrid), ("dt", C.c_double), ("buf", FlameStageBuffers),
+                ("metrics", FlameMetrics), ("thermo", FlameThermo),
+                ("transport", FlameTransport)]
+
+
 P = C.c_void_p
 G = C.POINTER(FlameGrid)
 S = C.c_void_p  # cudaStream_t
@@ -96,6 +102,11 @@ SIGNATURES = {
     "flame_rk_stage_noalloc": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
     "flame_transport": [G, S, P, P, P, TH, TR, I],
     "flame_stage_scratch_bytes": [G, I],
+    "flame_batch_workspace_bytes": [C.POINTER(FlameCaseDesc), I, I],
+    "flame_batch_create": [C.POINTER(C.c_void_p), C.POINTER(FlameCaseDesc), I, I, P, C.c_size_t,
+                           S],
+    "flame_batch_stage": [P, S, I, I],
+    "flame_batch_destroy": [P],
     "flame_last_error": [C.c_char_p, C.c_size_t],
     "flame_version": [],
 }
@@ -122,7 +133,7 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = C.c_size_t if name == "flame_stage_scratch_bytes" else C.c_int
+        fn.restype = C.c_size_t if name.endswith("_bytes") else C.c_int
     _LIB = lib
     return lib
 

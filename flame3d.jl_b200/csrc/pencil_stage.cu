@@ -20,6 +20,10 @@
 // Template parameters as in fused_stage.cu: NS species, QT storage of Q / transport, CT
 // arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
 
+#include <cstring>
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 
 namespace flame {
@@ -89,8 +93,8 @@ __device__ __forceinline__ CT ldg(const T *p, int i) {
 
 // ----------------------------------------------------------------------------------- prep
 template <int NS, typename QT>
-__global__ void __launch_bounds__(256) k_prep(const __grid_constant__ Args<QT> A) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prep_block(const Args<QT> &A, int bid) {
+    const int c = bid * 256 + threadIdx.x;
     if (c >= A.np) return;
     const int gx = c % A.tx, gy = (c / A.tx) % A.ty, gz = c / A.sz;
     const QT *P = A.Qi + 4 * A.np;
@@ -112,6 +116,11 @@ __global__ void __launch_bounds__(256) k_prep(const __grid_constant__ Args<QT> A
     const double rinv = 1 / jmax(double(A.Qi[c]), kEps);
 #pragma unroll
     for (int n = 0; n < NS; ++n) A.aux[c + (1 + n) * A.np] = QT(jmax(A.ri[c + n * A.np] * rinv, 0.0));
+}
+
+template <int NS, typename QT>
+__global__ void __launch_bounds__(256) k_prep(const __grid_constant__ Args<QT> A) {
+    prep_block<NS, QT>(A, blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------------- sweep
@@ -383,14 +392,13 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
 
 // x sweep (lanes along x, every access coalesced); it is the last sweep and finishes the stage.
 template <int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_constant__ Args<QT> A) {
+__device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned char *smem_raw) {
     constexpr int WPB = Wpb<0>::value;
     using SL = Slots<NS>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     CT *S = reinterpret_cast<CT *>(smem_raw) + warp * SL::N * 32;
     const int nseg = (A.nx + OWN - 1) / OWN;
-    const int gw = blockIdx.x * WPB + warp;
+    const int gw = bid * WPB + warp;
     const int seg = gw % nseg;
     const int y = (gw / nseg) % A.ny, z = (gw / nseg) / A.ny;
     if (z >= A.nz) return;
@@ -416,6 +424,12 @@ __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_co
     finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
 }
 
+template <int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_constant__ Args<QT> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    x_block<NS, QT, CT>(A, blockIdx.x, smem_raw);
+}
+
 // Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
 // use whole 128-byte lines; 8 when the column slots would not fit in shared memory.
 template <int NS, typename CT>
@@ -429,17 +443,15 @@ struct Staged {
 // exactly like the x sweep, and the right-hand side goes back with x-fastest threads.
 // PASS 0 writes R, PASS 1 adds to it.
 template <int DIR, int PASS, int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
-    k_pencil_staged(const __grid_constant__ Args<QT> A) {
+__device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsigned char *smem_raw) {
     constexpr int COLS = Staged<NS, CT>::COLS, STRIDE = Staged<NS, CT>::STRIDE;
     using SL = Slots<NS>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     CT *base = reinterpret_cast<CT *>(smem_raw);
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
     const int nseg = (n_along + OWN - 1) / OWN;
     const int nxb = (A.nx + COLS - 1) / COLS;
-    int bid = blockIdx.x;
+    int bid = block;
     const int xb = bid % nxb;
     bid /= nxb;
     const int seg = bid % nseg, c2 = bid / nseg;
@@ -484,6 +496,60 @@ __global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
         const double d = double(Sc[(SL::G + n) * 32 + l]) - double(Sc[(SL::G + n) * 32 + l + 1]);
         if (PASS == 0) A.R[g + n * A.np] = d;
         else A.R[g + n * A.np] += d;
+    }
+}
+
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
+    k_pencil_staged(const __grid_constant__ Args<QT> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    staged_block<DIR, PASS, NS, QT, CT>(A, blockIdx.x, smem_raw);
+}
+
+// ---------------------------------------------------------------------- batched, persistent
+// The same sweeps over many independent cases: a persistent grid walks a work list of
+// (case, block) items; off[c] is the first item of case c (off[n] = total).  Per-case
+// descriptors live in device memory.  Cases never read each other's data, so a case's result
+// does not depend on which other cases share the batch.
+__device__ __forceinline__ int case_of(const int *off, int n, int item) {
+    int lo = 0, hi = n - 1;  // largest c with off[c] <= item
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int NS, typename QT>
+__global__ void __launch_bounds__(256) k_prep_batch(const Args<QT> *cases, const int *off, int n) {
+    const int total = off[n];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int c = case_of(off, n, item);
+        prep_block<NS, QT>(cases[c], item - off[c]);
+    }
+}
+
+template <int DIR, int PASS, int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
+    k_staged_batch(const Args<QT> *cases, const int *off, int n) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int total = off[n];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int c = case_of(off, n, item);
+        staged_block<DIR, PASS, NS, QT, CT>(cases[c], item - off[c], smem_raw);
+        __syncthreads();  // the next item overwrites the staged columns
+    }
+}
+
+template <int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(Wpb<0>::value * 32)
+    k_x_batch(const Args<QT> *cases, const int *off, int n) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int total = off[n];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int c = case_of(off, n, item);
+        x_block<NS, QT, CT>(cases[c], item - off[c], smem_raw);
+        __syncwarp();  // each warp reuses only its own slots
     }
 }
 
@@ -604,4 +670,270 @@ extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
     const size_t np = (size_t)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
     const size_t q = precision == 0 ? sizeof(double) : sizeof(float);
     return np * ((5 + g->ns) * sizeof(double) + (1 + g->ns) * q);
+}
+
+// ============================================================================= batches
+// A batch advances many independent periodic cases per stage with the persistent kernels above:
+// per species count one group, per group and stage four launches (prep, z, y, x).  Descriptors
+// and work lists for the three stages and both in/out parities are uploaded once, into device
+// workspace the caller owns, so flame_batch_stage issues kernel launches only.
+namespace flame {
+namespace pencil {
+
+struct BatchGroup {
+    int ns = 0, n = 0;
+    const void *args[6] = {};  // device Args arrays, index (stage - 1) * 2 + parity
+    const int *off[4] = {};    // device work-list offsets: prep, z, y, x
+    int total[4] = {};
+    int grid[4] = {};          // persistent grid sizes
+};
+
+}  // namespace pencil
+}  // namespace flame
+
+struct FlameBatch {
+    int precision = 0;
+    int ngroups = 0;
+    flame::pencil::BatchGroup g[FLAME_MAX_NS];
+};
+
+namespace flame {
+namespace pencil {
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <typename QT>
+size_t args_size() { return sizeof(Args<QT>); }
+
+inline void case_items(const FlameGrid &g, int ns, int precision, int items[4]) {
+    const int tx = g.nx + 2 * g.ng, ty = g.ny + 2 * g.ng, tz = g.nz + 2 * g.ng;
+    const int np = tx * ty * tz;
+    int cols = 16;
+    // Staged<NS, CT>::COLS, evaluated on the host for the case's species count
+    const int nslot = 10 + 2 * ns + 4 + 10 + 3 + 1 + ns + 8 + 2 * ns + 1;
+    const size_t csz = precision == 0 ? 8 : 4;
+    if (csz * nslot * 33 * 16 > 200 * 1024) cols = 8;
+    const int nxb = (g.nx + cols - 1) / cols;
+    items[0] = (np + 255) / 256;
+    items[1] = nxb * ((g.nz + OWN - 1) / OWN) * g.ny;  // z sweep
+    items[2] = nxb * ((g.ny + OWN - 1) / OWN) * g.nz;  // y sweep
+    const long long warps = (long long)g.ny * g.nz * ((g.nx + OWN - 1) / OWN);
+    items[3] = (int)((warps + Wpb<0>::value - 1) / Wpb<0>::value);
+}
+
+template <int NS, typename QT, typename CT>
+int batch_grids(BatchGroup &bg) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    using ST = Staged<NS, CT>;
+    const size_t sm_st = sizeof(CT) * ST::STRIDE * ST::COLS;
+    const size_t sm_x = smem_bytes<NS, CT, Wpb<0>::value>();
+    static bool d0[64] = {}, d1[64] = {}, d2[64] = {};
+    if (int e = set_smem(k_staged_batch<2, 0, NS, QT, CT>, sm_st, d0)) return e;
+    if (int e = set_smem(k_staged_batch<1, 1, NS, QT, CT>, sm_st, d1)) return e;
+    if (int e = set_smem(k_x_batch<NS, QT, CT>, sm_x, d2)) return e;
+    int occ[4] = {0, 0, 0, 0};
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_prep_batch<NS, QT>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_staged_batch<2, 0, NS, QT, CT>,
+                                                  ST::COLS * 32, sm_st);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_staged_batch<1, 1, NS, QT, CT>,
+                                                  ST::COLS * 32, sm_st);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_x_batch<NS, QT, CT>,
+                                                  Wpb<0>::value * 32, sm_x);
+    for (int k = 0; k < 4; ++k) {
+        const int cap = sms * (occ[k] > 0 ? occ[k] : 1);
+        bg.grid[k] = bg.total[k] < cap ? bg.total[k] : cap;
+        if (bg.grid[k] < 1) bg.grid[k] = 1;
+    }
+    return flame_check_launch("flame_batch_create");
+}
+
+template <int NS, typename QT, typename CT>
+int batch_launch(const BatchGroup &bg, cudaStream_t s, int stage, int parity) {
+    const Args<QT> *a = static_cast<const Args<QT> *>(bg.args[(stage - 1) * 2 + parity]);
+    using ST = Staged<NS, CT>;
+    const size_t sm_st = sizeof(CT) * ST::STRIDE * ST::COLS;
+    const size_t sm_x = smem_bytes<NS, CT, Wpb<0>::value>();
+    k_prep_batch<NS, QT><<<bg.grid[0], 256, 0, s>>>(a, bg.off[0], bg.n);
+    k_staged_batch<2, 0, NS, QT, CT><<<bg.grid[1], ST::COLS * 32, sm_st, s>>>(a, bg.off[1], bg.n);
+    k_staged_batch<1, 1, NS, QT, CT><<<bg.grid[2], ST::COLS * 32, sm_st, s>>>(a, bg.off[2], bg.n);
+    k_x_batch<NS, QT, CT><<<bg.grid[3], Wpb<0>::value * 32, sm_x, s>>>(a, bg.off[3], bg.n);
+    return flame_check_launch("flame_batch_stage");
+}
+
+template <typename QT, typename CT>
+int batch_dispatch(int what, BatchGroup &bg, cudaStream_t s, int stage, int parity) {
+    switch (bg.ns) {
+#define CASE(N)                                                             \
+    case N:                                                                 \
+        return what == 0 ? batch_grids<N, QT, CT>(bg)                       \
+                         : batch_launch<N, QT, CT>(bg, s, stage, parity);
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
+#undef CASE
+        default:
+            return flame_fail(FLAME_EUNSUPPORTED, "flame_batch: ns=%d (1..9)", bg.ns);
+    }
+}
+
+template <typename QT>
+void fill_args(std::vector<unsigned char> &host, size_t at, const FlameCaseDesc &c, int stage,
+               int parity) {
+    FlameStageBuffers b = c.buf;
+    if (parity) {  // the stage reads what the buffers call "out" and writes "in"
+        const void *q = b.Q_in, *t = b.trans_in;
+        const double *r = b.rhoi_in;
+        b.Q_in = b.Q_out, b.Q_out = const_cast<void *>(q);
+        b.rhoi_in = b.rhoi_out, b.rhoi_out = const_cast<double *>(r);
+        b.trans_in = b.trans_out, b.trans_out = const_cast<void *>(t);
+    }
+    const Args<QT> A =
+        make_args<QT>(c.grid, stage, c.dt, b, c.metrics, c.thermo, c.transport, c.buf.scratch);
+    memcpy(host.data() + at, &A, sizeof(A));
+}
+
+}  // namespace pencil
+}  // namespace flame
+
+namespace {
+
+// Group sizes and the byte layout of the workspace: per group, six descriptor arrays then four
+// work-list offset arrays, each aligned to 256 bytes.
+struct Layout {
+    int ngroups = 0;
+    int ns[FLAME_MAX_NS] = {}, count[FLAME_MAX_NS] = {};
+    size_t args_at[FLAME_MAX_NS][6] = {}, off_at[FLAME_MAX_NS][4] = {};
+    size_t bytes = 0;
+};
+
+int plan_layout(const FlameCaseDesc *cases, int n, int precision, Layout &L) {
+    for (int i = 0; i < n; ++i) {
+        const int ns = cases[i].grid.ns;
+        int k = 0;
+        while (k < L.ngroups && L.ns[k] != ns) ++k;
+        if (k == L.ngroups) {
+            if (L.ngroups == FLAME_MAX_NS) return flame_fail(FLAME_EINVAL, "flame_batch: groups");
+            L.ns[L.ngroups++] = ns;
+        }
+        ++L.count[k];
+    }
+    const size_t asz = precision == 0 ? flame::pencil::args_size<double>()
+                                      : flame::pencil::args_size<float>();
+    size_t at = 0;
+    for (int k = 0; k < L.ngroups; ++k) {
+        for (int v = 0; v < 6; ++v) L.args_at[k][v] = at, at = flame::pencil::align256(at + asz * L.count[k]);
+        for (int w = 0; w < 4; ++w)
+            L.off_at[k][w] = at, at = flame::pencil::align256(at + sizeof(int) * (L.count[k] + 1));
+    }
+    L.bytes = at;
+    return FLAME_OK;
+}
+
+int check_case(const FlameCaseDesc &c, int i) {
+    if (int e = flame_check_grid(&c.grid, "flame_batch")) return e;
+    if ((c.grid.periodic & 7) != 7)
+        return flame_fail(FLAME_EUNSUPPORTED, "flame_batch: case %d is not periodic", i);
+    if (c.grid.ns > 9) return flame_fail(FLAME_EUNSUPPORTED, "flame_batch: case %d ns > 9", i);
+    if (c.grid.nx < FLAME_NG || c.grid.ny < FLAME_NG || c.grid.nz < FLAME_NG)
+        return flame_fail(FLAME_EINVAL, "flame_batch: case %d extents must be >= %d", i, FLAME_NG);
+    const long long np =
+        (long long)(c.grid.nx + 8) * (c.grid.ny + 8) * (c.grid.nz + 8);
+    if (np * 10 >= (1LL << 31)) return flame_fail(FLAME_EINVAL, "flame_batch: case %d too large", i);
+    const FlameStageBuffers &b = c.buf;
+    if (!b.U || !b.Un || !b.Q_in || !b.Q_out || !b.rhoi_in || !b.rhoi_out || !b.rhon ||
+        !b.trans_in || !b.trans_out || !b.scratch || !c.metrics.J || !c.metrics.dxidx)
+        return flame_fail(FLAME_EINVAL, "flame_batch: case %d has a NULL buffer", i);
+    if (c.transport.law != 0 && c.transport.law != 1)
+        return flame_fail(FLAME_EINVAL, "flame_batch: case %d transport law", i);
+    return FLAME_OK;
+}
+
+}  // namespace
+
+extern "C" size_t flame_batch_workspace_bytes(const FlameCaseDesc *cases, int n, int precision) {
+    if (!cases || n < 1) return 0;
+    Layout L;
+    if (plan_layout(cases, n, precision, L)) return 0;
+    return L.bytes;
+}
+
+extern "C" int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, int n,
+                                  int precision, void *workspace, size_t bytes,
+                                  flame_stream_t s) {
+    if (!out || !cases || n < 1) return flame_fail(FLAME_EINVAL, "flame_batch_create: no cases");
+    if (precision != 0 && precision != 1)
+        return flame_fail(FLAME_EINVAL, "flame_batch_create: precision=%d", precision);
+    for (int i = 0; i < n; ++i)
+        if (int e = check_case(cases[i], i)) return e;
+    Layout L;
+    if (int e = plan_layout(cases, n, precision, L)) return e;
+    if (!workspace || bytes < L.bytes)
+        return flame_fail(FLAME_EINVAL, "flame_batch_create: workspace of %zu bytes, need %zu",
+                          bytes, L.bytes);
+    std::vector<unsigned char> host(L.bytes, 0);
+    FlameBatch *B = new FlameBatch();
+    B->precision = precision;
+    B->ngroups = L.ngroups;
+    unsigned char *dev = static_cast<unsigned char *>(workspace);
+    const size_t asz = precision == 0 ? flame::pencil::args_size<double>()
+                                      : flame::pencil::args_size<float>();
+    for (int k = 0; k < L.ngroups; ++k) {
+        flame::pencil::BatchGroup &bg = B->g[k];
+        bg.ns = L.ns[k];
+        bg.n = L.count[k];
+        std::vector<int> off[4];
+        for (int w = 0; w < 4; ++w) off[w].push_back(0);
+        int j = 0;
+        for (int i = 0; i < n; ++i) {
+            if (cases[i].grid.ns != bg.ns) continue;
+            for (int st = 1; st <= 3; ++st)
+                for (int par = 0; par < 2; ++par) {
+                    const size_t at = L.args_at[k][(st - 1) * 2 + par] + asz * j;
+                    if (precision == 0) flame::pencil::fill_args<double>(host, at, cases[i], st, par);
+                    else flame::pencil::fill_args<float>(host, at, cases[i], st, par);
+                }
+            int items[4];
+            flame::pencil::case_items(cases[i].grid, bg.ns, precision, items);
+            for (int w = 0; w < 4; ++w) off[w].push_back(off[w].back() + items[w]);
+            ++j;
+        }
+        for (int w = 0; w < 4; ++w) {
+            memcpy(host.data() + L.off_at[k][w], off[w].data(), sizeof(int) * off[w].size());
+            bg.off[w] = reinterpret_cast<const int *>(dev + L.off_at[k][w]);
+            bg.total[w] = off[w].back();
+        }
+        for (int v = 0; v < 6; ++v) bg.args[v] = dev + L.args_at[k][v];
+        const int e = precision == 0 ? flame::pencil::batch_dispatch<double, double>(0, bg, s, 1, 0)
+                                     : flame::pencil::batch_dispatch<float, float>(0, bg, s, 1, 0);
+        if (e) {
+            delete B;
+            return e;
+        }
+    }
+    cudaError_t ce = cudaMemcpyAsync(workspace, host.data(), L.bytes, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) {
+        delete B;
+        return flame_fail(FLAME_ELAUNCH, "flame_batch_create: upload: %s", cudaGetErrorString(ce));
+    }
+    *out = B;
+    return FLAME_OK;
+}
+
+extern "C" int flame_batch_stage(FlameBatch *B, flame_stream_t s, int stage, int parity) {
+    if (!B) return flame_fail(FLAME_EINVAL, "flame_batch_stage: NULL batch");
+    if (stage < 1 || stage > 3 || (parity != 0 && parity != 1))
+        return flame_fail(FLAME_EINVAL, "flame_batch_stage: stage=%d parity=%d", stage, parity);
+    for (int k = 0; k < B->ngroups; ++k) {
+        const int e = B->precision == 0
+                          ? flame::pencil::batch_dispatch<double, double>(1, B->g[k], s, stage, parity)
+                          : flame::pencil::batch_dispatch<float, float>(1, B->g[k], s, stage, parity);
+        if (e) return e;
+    }
+    return FLAME_OK;
+}
+
+extern "C" int flame_batch_destroy(FlameBatch *B) {
+    delete B;
+    return FLAME_OK;
 }

@@ -249,6 +249,33 @@ int flame_transport(const FlameGrid *g, flame_stream_t stream, const void *Q, co
                     void *trans, const FlameThermo *thermo, const FlameTransport *transport,
                     int precision);
 
+/* ---------------------------------------------------------------------------------------
+ * Batches (no reference counterpart): many independent periodic cases, each with its own
+ * grid, species count, thermodynamics, transport, dt and buffers, advanced together by the
+ * pencil-sweep kernels.  A persistent grid per species-count group walks a (case, block) work
+ * list; one stage is four launches per group.  Descriptors and work lists for all stages and
+ * both in/out parities go once into caller-owned device workspace, so a captured CUDA graph of
+ * flame_batch_stage calls replays without host work.  parity 0 advances buf.*_in -> buf.*_out,
+ * parity 1 the other way.  Every case needs buf.scratch (flame_stage_scratch_bytes).  A case's
+ * result is the same as when it runs alone: cases share no data and no reduction.
+ * ------------------------------------------------------------------------------------- */
+typedef struct FlameCaseDesc {
+    FlameGrid grid;
+    double dt;
+    FlameStageBuffers buf;
+    FlameMetrics metrics;
+    FlameThermo thermo;
+    FlameTransport transport;
+} FlameCaseDesc;
+
+typedef struct FlameBatch FlameBatch; /* opaque host-side plan */
+
+size_t flame_batch_workspace_bytes(const FlameCaseDesc *cases, int n, int precision);
+int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, int n, int precision,
+                       void *workspace, size_t bytes, flame_stream_t stream);
+int flame_batch_stage(FlameBatch *batch, flame_stream_t stream, int stage, int parity);
+int flame_batch_destroy(FlameBatch *batch);
+
 /* Message of the last error on the calling thread; returns its length. */
 int flame_last_error(char *buf, size_t n);
 

@@ -1,0 +1,97 @@
+"""Batched stages (flame_batch_*): parity with the oracle, alone-vs-mix equality, graph replay."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix(f3d):
+    return [f3d.taylor_green(n=16),
+            f3d.random_curvilinear(n=12, ns=2, seed=51),
+            f3d.random_curvilinear(n=10, ns=1, seed=52),
+            f3d.taylor_green(n=12, ns=3, perturb=0.02, seed=53),
+            f3d.curvilinear_jet(nx=24, ny=16, nz=12, pressure_noise=0.02)]
+
+
+def _state(dc):
+    U = dc.conserved()
+    Q, r = dc.primitives()
+    return U, Q, r
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_matches_oracle(f3d, oracle, cuda_ok, precision):
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)
+    dcs = [S.DeviceCase(c, precision=precision, tile=3) for c in cases]
+    batch = B.Batch(dcs)
+    ocs = [oracle.OracleCase(c) for c in cases]
+    for _ in range(2):
+        batch.step()
+        for oc in ocs:
+            oc.step()
+    tol = 1e-12 if precision == 0 else 1e-5
+    I = oracle.interior
+    for dc, oc, c in zip(dcs, ocs, cases):
+        U = dc.conserved()
+        mom = np.linalg.norm(I(oc.U[1:4]).ravel())
+        for n in range(5):
+            ref = I(oc.U[n])
+            scale = mom if 1 <= n <= 3 else np.linalg.norm(ref.ravel())
+            err = np.linalg.norm((I(U[n]) - ref).ravel()) / scale
+            assert err <= tol, (c.name, n, err)
+    batch.close()
+
+
+def test_alone_equals_in_mix_bitwise(f3d, cuda_ok):
+    """A case's result does not depend on the other cases of its batch."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)
+    alone = S.DeviceCase(cases[1], precision=1, tile=3)
+    b1 = B.Batch([alone])
+    mixed = [S.DeviceCase(c, precision=1, tile=3) for c in cases]
+    b2 = B.Batch(mixed)
+    for _ in range(3):
+        b1.step()
+        b2.step()
+    for a, m in zip(_state(alone), _state(mixed[1])):
+        assert np.array_equal(a, m)
+    b1.close()
+    b2.close()
+
+
+def test_graph_replay_equals_launches(f3d, cuda_ok):
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)
+    d1 = [S.DeviceCase(c, tile=3) for c in cases]
+    d2 = [S.DeviceCase(c, tile=3) for c in cases]
+    b1, b2 = B.Batch(d1), B.Batch(d2)
+    b2.capture()
+    for _ in range(3):  # both parities of the captured graphs
+        b1.step()
+        b2.step()
+    for x, y in zip(d1, d2):
+        for a, b in zip(_state(x), _state(y)):
+            assert np.array_equal(a, b)
+    b1.close()
+    b2.close()
+
+
+def test_batch_agrees_with_single_case_path(f3d, cuda_ok):
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    case = f3d.random_curvilinear(n=12, ns=3, seed=54)
+    single = S.DeviceCase(case, tile=3)
+    batched = S.DeviceCase(case, tile=3)
+    b = B.Batch([batched])
+    single.step()
+    b.step()
+    for a, c in zip(_state(single), _state(batched)):
+        n = np.linalg.norm(a.ravel())
+        assert np.linalg.norm((a - c).ravel()) <= 1e-13 * n
+    b.close()
