@@ -1,9 +1,16 @@
-"""Batched stages: many resident cases advanced together (flame_batch_* in the C ABI).
+"""Batched stages: many resident cases advanced together.
 
 A `Batch` groups `DeviceCase`s that use the pencil configuration (each owns its state, metrics
-and scratch).  One stage is a few persistent launches per species-count group, whatever the
-number of cases; `capture()` records one RK3 step per in/out parity as CUDA graphs so the
-serving loop replays a whole step with one graph launch.
+and scratch).  Two modes:
+
+* "persistent": flame_batch_* in the C ABI; one stage is four persistent launches per
+  species-count group over a (case, block) work list, whatever the number of cases;
+* "graph": every case's own launch chain (prep, z, y, x sweeps per stage) on one of several
+  streams, forked and joined inside one CUDA graph, so the chains of small cases run side by
+  side on the GPU and every kernel keeps its parameters in the constant bank.
+
+`capture()` records one RK3 step per in/out parity as CUDA graphs, so the serving loop replays a
+whole step of every case with one graph launch.
 """
 from __future__ import annotations
 
@@ -20,7 +27,8 @@ def _p(t):
 
 
 class Batch:
-    def __init__(self, cases: list, device: str | torch.device = "cuda"):
+    def __init__(self, cases: list, device: str | torch.device = "cuda", mode: str = "graph",
+                 streams: int = 16):
         if not cases:
             raise abi.FlameError(1, "a batch needs at least one case")
         self.lib = abi.load_library()
@@ -33,6 +41,17 @@ class Batch:
         for dc in self.cases:
             if dc.tile != 3 or dc.scratch is None:
                 raise abi.FlameError(1, "batched cases use the pencil configuration (tile=3)")
+        self.mode = mode
+        self.parity = 0
+        self.graphs: dict[int, torch.cuda.CUDAGraph] = {}
+        self.handle = None
+        if mode == "graph":
+            # largest cases first, dealt round-robin over the streams
+            self.order = sorted(range(len(self.cases)), key=lambda k: -self.cases[k].case.cells)
+            self.side = [torch.cuda.Stream(self.device) for _ in range(min(streams, len(cases)))]
+            return
+        if mode != "persistent":
+            raise abi.FlameError(1, f"unknown batch mode {mode!r}")
         n = len(self.cases)
         descs = (FlameCaseDesc * n)()
         for k, dc in enumerate(self.cases):
@@ -54,8 +73,6 @@ class Batch:
                                          _p(self.workspace), nbytes, C.c_void_p(self.stream))
         abi.check(self.lib, rc)
         self.handle = h
-        self.parity = 0
-        self.graphs: dict[int, torch.cuda.CUDAGraph] = {}
 
     @property
     def stream(self) -> int:
@@ -69,12 +86,38 @@ class Batch:
         rc = self.lib.flame_batch_stage(self.handle, C.c_void_p(self.stream), stage, parity)
         abi.check(self.lib, rc)
 
+    def _fork_step(self) -> None:
+        """One RK3 step of every case, each case's chain on a side stream (flips every cur)."""
+        main = torch.cuda.current_stream(self.device)
+        ev = torch.cuda.Event()
+        ev.record(main)
+        for j, k in enumerate(self.order):
+            st = self.side[j % len(self.side)]
+            st.wait_event(ev)
+            with torch.cuda.stream(st):
+                self.cases[k].step()
+        for st in self.side:
+            main.wait_stream(st)
+
     def _flip(self) -> None:
         self.parity ^= 1
         for dc in self.cases:
             dc.cur = 1 - dc.cur
 
     def stage(self, stage: int) -> None:
+        if self.mode == "graph":
+            main = torch.cuda.current_stream(self.device)
+            ev = torch.cuda.Event()
+            ev.record(main)
+            for j, k in enumerate(self.order):
+                st = self.side[j % len(self.side)]
+                st.wait_event(ev)
+                with torch.cuda.stream(st):
+                    self.cases[k].stage_fused(stage)  # flips the case's cur
+            for st in self.side:
+                main.wait_stream(st)
+            self.parity ^= 1
+            return
         self._launch(stage, self.parity)
         self._flip()
 
@@ -86,12 +129,27 @@ class Batch:
             for _ in range(3):
                 self._flip()
             return
+        if self.mode == "graph":
+            self._fork_step()  # DeviceCase.step flips each case's cur
+            self.parity ^= 1
+            return
         for s in (1, 2, 3):
             self.stage(s)
 
     def capture(self) -> None:
         """Records one RK3 step for each starting parity as a CUDA graph."""
         torch.cuda.synchronize(self.device)
+        if self.mode == "graph":
+            start = self.parity
+            for par in (start, start ^ 1):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, capture_error_mode="thread_local"):
+                    self._fork_step()  # records the pointers of this parity, flips every cur
+                self.parity ^= 1
+                self.graphs[par] = g
+            # capturing launched nothing: both flips are undone, the state is unchanged
+            torch.cuda.synchronize(self.device)
+            return
         for par in (0, 1):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, capture_error_mode="thread_local"):

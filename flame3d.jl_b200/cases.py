@@ -136,11 +136,15 @@ def ghosted(nx: int, ny: int, nz: int) -> tuple[int, int, int]:
 
 
 def periodic_fill(a: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
-    """Copies every ghost of a (nv, Tz, Ty, Tx) array from its periodic image, in place."""
-    ix = NG + (np.arange(nx + 2 * NG) - NG) % nx
-    iy = NG + (np.arange(ny + 2 * NG) - NG) % ny
-    iz = NG + (np.arange(nz + 2 * NG) - NG) % nz
-    a[...] = a[:, iz][:, :, iy][:, :, :, ix]
+    """Copies every ghost of a (nv, Tz, Ty, Tx) array from its periodic image, in place
+    (axis by axis, so edges and corners come from the images already filled)."""
+    for ax, n in ((3, nx), (2, ny), (1, nz)):
+        def sl(lo, hi):
+            idx = [slice(None)] * 4
+            idx[ax] = slice(lo, hi)
+            return tuple(idx)
+        a[sl(0, NG)] = a[sl(n, n + NG)]
+        a[sl(n + NG, n + 2 * NG)] = a[sl(NG, 2 * NG)]
     return a
 
 
@@ -297,7 +301,7 @@ def taylor_green(n: int = 64, Re: float = 1600.0, Ma: float = 0.1, ns: int = 1,
     U0 = Ma sqrt(γ R T0), ρ = p/(R T0), μ = ρ0 U0 L / Re (L = 1), λ = cp μ / Pr (Pr = 0.71).
     With ns > 1 the gas is a uniform random mixture of the synthetic species; `perturb` adds
     random-phase Fourier modes with |k| <= 8 of that relative amplitude to u, v, w."""
-    thermo = ideal_air() if ns == 1 else synthetic_species(max(ns, 1), species_seed).subset(ns)
+    thermo = ideal_air() if ns == 1 else synthetic_species(9, species_seed).subset(ns)
     rng = np.random.default_rng(seed)
     Y = np.ones(1) if ns == 1 else rng.dirichlet(np.ones(ns))
     h = 2 * math.pi / n
@@ -330,7 +334,10 @@ def taylor_green(n: int = 64, Re: float = 1600.0, Ma: float = 0.1, ns: int = 1,
 
 
 def _fourier_noise(rng, X, Y, Z, kmax=8, nmodes=24):
-    """Sum of random-phase modes with integer wavenumbers |k| <= kmax, unit max amplitude."""
+    """Sum of random-phase modes with integer wavenumbers |k| <= kmax, unit max amplitude.
+    X, Y, Z are the meshgrid of a uniform periodic axis; each mode is the imaginary part of an
+    outer product of three 1-D complex exponentials."""
+    x, y, z = X[0, 0, :], Y[0, :, 0], Z[:, 0, 0]
     acc = np.zeros_like(X)
     for _ in range(nmodes):
         while True:
@@ -338,8 +345,28 @@ def _fourier_noise(rng, X, Y, Z, kmax=8, nmodes=24):
             if 0 < np.linalg.norm(k) <= kmax:
                 break
         ph = rng.uniform(0, 2 * math.pi)
-        acc += np.sin(k[0] * X + k[1] * Y + k[2] * Z + ph)
+        ex, ey, ez = np.exp(1j * k[0] * x), np.exp(1j * k[1] * y), np.exp(1j * (k[2] * z + ph))
+        acc += (ez[:, None, None] * ey[None, :, None] * ex[None, None, :]).imag
     return acc / nmodes
+
+
+def ensemble(n_cases: int = 64, seed: int = 4, sizes=(32, 48, 64, 96, 128),
+             species_seed: int = 3) -> list:
+    """The batched benchmark ensemble: independent periodic Taylor-Green cases with sizes drawn
+    uniformly from `sizes` (cubes), Re ~ U[400, 3200], Ma ~ U[0.1, 0.5], 1-9 species from the
+    synthetic set, plus 2 % random-phase Fourier modes with |k| <= 8 (seeded per case)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_cases):
+        n = int(rng.choice(sizes))
+        Re = float(rng.uniform(400, 3200))
+        Ma = float(rng.uniform(0.1, 0.5))
+        ns = int(rng.integers(1, 10))
+        c = taylor_green(n=n, Re=Re, Ma=Ma, ns=ns, perturb=0.02, seed=seed * 1000 + i,
+                         species_seed=species_seed)
+        c.name = f"ens{i:02d}_tgv{n}_ns{ns}"
+        out.append(c)
+    return out
 
 
 def curvilinear_jet(nx: int = 256, ny: int = 128, nz: int = 128, seed: int = 1,

@@ -21,13 +21,17 @@ def _state(dc):
     return U, Q, r
 
 
+MODES = ["persistent", "graph"]
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("precision", [0, 1])
-def test_batch_matches_oracle(f3d, oracle, cuda_ok, precision):
+def test_batch_matches_oracle(f3d, oracle, cuda_ok, precision, mode):
     S = f3d.solver_module()
     B = f3d.batch_module()
     cases = _mix(f3d)
     dcs = [S.DeviceCase(c, precision=precision, tile=3) for c in cases]
-    batch = B.Batch(dcs)
+    batch = B.Batch(dcs, mode=mode)
     ocs = [oracle.OracleCase(c) for c in cases]
     for _ in range(2):
         batch.step()
@@ -46,15 +50,17 @@ def test_batch_matches_oracle(f3d, oracle, cuda_ok, precision):
     batch.close()
 
 
-def test_alone_equals_in_mix_bitwise(f3d, cuda_ok):
+@pytest.mark.parametrize("mode", MODES)
+def test_alone_equals_in_mix_bitwise(f3d, cuda_ok, mode):
     """A case's result does not depend on the other cases of its batch."""
     S = f3d.solver_module()
     B = f3d.batch_module()
     cases = _mix(f3d)
     alone = S.DeviceCase(cases[1], precision=1, tile=3)
-    b1 = B.Batch([alone])
+    b1 = B.Batch([alone], mode=mode)
     mixed = [S.DeviceCase(c, precision=1, tile=3) for c in cases]
-    b2 = B.Batch(mixed)
+    b2 = B.Batch(mixed, mode=mode)
+    b2.capture()
     for _ in range(3):
         b1.step()
         b2.step()
@@ -64,13 +70,16 @@ def test_alone_equals_in_mix_bitwise(f3d, cuda_ok):
     b2.close()
 
 
-def test_graph_replay_equals_launches(f3d, cuda_ok):
+@pytest.mark.parametrize("mode", MODES)
+def test_graph_replay_equals_launches(f3d, cuda_ok, mode):
     S = f3d.solver_module()
     B = f3d.batch_module()
     cases = _mix(f3d)
     d1 = [S.DeviceCase(c, tile=3) for c in cases]
     d2 = [S.DeviceCase(c, tile=3) for c in cases]
-    b1, b2 = B.Batch(d1), B.Batch(d2)
+    b1, b2 = B.Batch(d1, mode=mode), B.Batch(d2, mode=mode)
+    b1.stage(1)  # a single stage first, so the graphs start from the odd parity
+    b2.stage(1)
     b2.capture()
     for _ in range(3):  # both parities of the captured graphs
         b1.step()
