@@ -68,6 +68,8 @@ WORKLOADS = {
     "tgv64": dict(kind="tgv", n=64),
     "mix192_ns9": dict(kind="mixing", n=192, ns=9),
     "ensemble64": dict(kind="ensemble"),
+    "serve": dict(kind="serve"),
+    "precision": dict(kind="precision"),
 }
 
 
@@ -170,6 +172,8 @@ def run_reference(args, f3d):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     lib = oracle.load()
+    if WORKLOADS[args.workload]["kind"] not in ("jet", "tgv", "mixing"):
+        args.workload = "jet256x128x128"  # case-set workloads: the reference RHS on the jet
     w = WORKLOADS[args.workload]
     nz = 16 if w["kind"] == "jet" else None
     case = make_case(f3d, args.workload, nz_override=nz) if nz else make_case(f3d, args.workload)
@@ -273,6 +277,127 @@ def run_ensemble(args, f3d) -> int:
     return 0
 
 
+def _conserved_errors(U, Uref, interior) -> dict:
+    """Relative L2 of ρ, ρu (the momentum vector field) and ρE."""
+    import numpy as np
+    I = interior
+    rel = lambda a, b, n: float(np.linalg.norm((I(a) - I(b)).ravel()) / n)  # noqa: E731
+    mom = np.linalg.norm(I(Uref[1:4]).ravel())
+    return {"rho": rel(U[0], Uref[0], np.linalg.norm(I(Uref[0]).ravel())),
+            "rhou": rel(U[1:4], Uref[1:4], mom),
+            "rhoE": rel(U[4], Uref[4], np.linalg.norm(I(Uref[4]).ravel()))}
+
+
+def run_precision(args, f3d) -> int:
+    """Error of the mixed-precision path after 1000 RK3 steps.  Full-size configurations: mixed
+    against the plain FP64 path on the GPU (itself within 1e-12 of the oracle in the parity
+    tests).  Small cases: both GPU paths against the FP64 oracle on the host cores."""
+    import numpy as np
+
+    import torch
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    S = f3d.solver_module()
+    steps = args.precision_steps
+    I = oracle.interior
+    out = {"steps": steps, "full_size": {}, "vs_oracle": {}}
+    full = [("tgv64", f3d.taylor_green(n=64)), ("jet256x128x128", f3d.curvilinear_jet()),
+            ("mix192_ns9", f3d.mixing_layer(n=192, ns=9))]
+    for name, case in full:
+        res = {}
+        for prec in (0, 1):
+            dc = S.DeviceCase(case, device=dev, precision=prec, tile=3)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                dc.step()
+            torch.cuda.synchronize(dev)
+            res[prec] = (dc.conserved(), time.perf_counter() - t0)
+            del dc
+            torch.cuda.empty_cache()
+        out["full_size"][name] = {"mixed_vs_fp64": _conserved_errors(res[1][0], res[0][0], I),
+                                  "finite": bool(np.isfinite(res[1][0]).all()),
+                                  "seconds": {"fp64": res[0][1], "mixed": res[1][1]}}
+        print(json.dumps({name: out["full_size"][name]}), flush=True)
+    small = [("tgv32", f3d.taylor_green(n=32)),
+             ("jet64x32x32", f3d.curvilinear_jet(nx=64, ny=32, nz=32)),
+             ("mix32_ns9", f3d.mixing_layer(n=32, ns=9))]
+    for name, case in small:
+        oc = oracle.OracleCase(case)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            oc.step()
+        t_or = time.perf_counter() - t0
+        errs = {}
+        for prec, label in ((0, "fp64"), (1, "mixed")):
+            dc = S.DeviceCase(case, device=dev, precision=prec, tile=3)
+            for _ in range(steps):
+                dc.step()
+            errs[label] = _conserved_errors(dc.conserved(), oc.U, I)
+            del dc
+        out["vs_oracle"][name] = {**errs, "oracle_seconds": t_or}
+        print(json.dumps({name: out["vs_oracle"][name]}), flush=True)
+    print(json.dumps({"workload": "precision", **out}), flush=True)
+    return 0
+
+
+def run_serve(args, f3d) -> int:
+    """The serving stream: seeded Poisson arrivals (λ = 20/s) of solve requests with n
+    log-uniform over 32-256, Cartesian or curvilinear, 1-9 species, Re 400-3200, Ma 0.1-1.5
+    and 200-2000 RK3 steps scaled by --step-scale, admitted against a 150 GB HBM budget and
+    served with continuous batching in mixed precision; against the same requests one at a time
+    in arrival order with the plain FP64 stage.  Wall-clock makespan from the first arrival to
+    the last completion (case construction on the device and result download included)."""
+    import importlib
+
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    S = importlib.import_module(f3d.__name__ + ".serving")
+    reqs = S.request_stream(args.requests, rate=20.0, seed=5, step_scale=args.step_scale)
+    warm = S.request_stream(3, rate=1000.0, seed=6, n_range=(16, 24), steps_range=(2, 3))
+    S.fifo(warm, dev, precision=0)  # module loads, allocator, graph pools
+    S.Server(dev, precision=1).run(warm)
+    torch.cuda.synchronize(dev)
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    clk = ClockSampler(f"GPU-{uuid}" if uuid else None)
+    clk.start()
+    time.sleep(0.3)
+    base = S.fifo(reqs, dev, precision=0)
+    torch.cuda.empty_cache()
+    srv = S.Server(dev, precision=1, hbm_budget=150e9)
+    rep = srv.run(reqs)
+    clocks = clk.stop()
+    if args.serve_log:
+        with open(args.serve_log, "w") as fh:
+            for arm, r in (("fifo_fp64", base), ("serving_mixed", rep)):
+                for pr in r["per_request"]:
+                    fh.write(json.dumps({"arm": arm, **pr}) + "\n")
+    drop = ("per_request",)
+    summ = lambda r: {k: v for k, v in r.items() if k not in drop}  # noqa: E731
+    value = rep["mcell_stage_per_s"]
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+           "steps": rep["step_latency_ms"]["steps"], "warmup": 3,
+           "ms_per_step": rep["step_latency_ms"]["p50"], "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+           "data": "synthetic (seeded Poisson request stream, Taylor-Green initial states "
+                   "built on the device)",
+           "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": 20.0,
+                      "seed": 5, "step_scale": args.step_scale, "hbm_budget_bytes": 150e9,
+                      "cell_stages": sum(r.cell_stages for r in reqs),
+                      "path": "continuous batching, graph-mode batch, mixed precision",
+                      "l2": "inputs of the large cases exceed L2; no flush between steps"},
+           "step_latency_ms": rep["step_latency_ms"],
+           "completion_latency_s": rep["completion_latency_s"],
+           "serving": summ(rep), "plain_fp64_fifo": summ(base),
+           "speedup_vs_plain_fp64_fifo": value / base["mcell_stage_per_s"],
+           "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------------------ GPU side
 def main() -> int:
     ap = argparse.ArgumentParser()
@@ -286,6 +411,12 @@ def main() -> int:
     ap.add_argument("--tile", type=int, default=None,
                     help="stage configuration (0-3); default: the autotuner's choice")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests in the stream")
+    ap.add_argument("--step-scale", type=float, default=0.05,
+                    help="serve: factor on the requested 200-2000 steps")
+    ap.add_argument("--serve-log", default=None, help="serve: per-request JSON lines to this file")
+    ap.add_argument("--precision-steps", type=int, default=1000,
+                    help="precision: RK3 steps before the errors are measured")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     f3d = _package()
@@ -293,6 +424,10 @@ def main() -> int:
         return run_reference(args, f3d)
     if args.workload == "ensemble64":
         return run_ensemble(args, f3d)
+    if args.workload == "serve":
+        return run_serve(args, f3d)
+    if args.workload == "precision":
+        return run_precision(args, f3d)
 
     import torch
     import torch.distributed as dist

@@ -54,19 +54,26 @@ class Thermo:
                       self.sep[:ns].copy(), self.min_temp, self.max_temp, self.Ru)
 
     # Host evaluations with the reference's formulas (thermo.jl), vectorised over points.
-    def internal_energy(self, T: np.ndarray, rhoi: np.ndarray) -> np.ndarray:
-        """InternalEnergy (thermo.jl:219-228), J/m^3; rhoi has shape (ns, ...)."""
+    def species_energy(self, T: np.ndarray) -> list[np.ndarray]:
+        """Per species e_n(T) R_u^-1 W_n (the polynomial of InternalEnergy, thermo.jl:219-228)."""
         T2 = 0.5 * T * T
         T3 = 2.0 / 3.0 * T2 * T
         T4 = T2 * T2
         T5 = 0.8 * T4 * T
-        r = np.zeros_like(T)
+        out = []
         for n in range(self.ns):
             lo, hi = self.lo[n], self.hi[n]
             e_lo = (lo[0] - 1) * T + lo[1] * T2 + lo[2] * T3 + lo[3] * T4 + lo[4] * T5
             e_hi = ((hi[0] - 1) * T + hi[1] * T2 + hi[2] * T3 + hi[3] * T4 + hi[4] * T5
                     + (hi[5] - lo[5]))
-            r = r + rhoi[n] * np.where(T < self.sep[n], e_lo, e_hi) / self.mw[n]
+            out.append(np.where(T < self.sep[n], e_lo, e_hi))
+        return out
+
+    def internal_energy(self, T: np.ndarray, rhoi: np.ndarray) -> np.ndarray:
+        """InternalEnergy (thermo.jl:219-228), J/m^3; rhoi has shape (ns, ...)."""
+        r = np.zeros_like(T)
+        for n, e in enumerate(self.species_energy(T)):
+            r = r + rhoi[n] * e / self.mw[n]
         return r * self.Ru
 
     def cp_mass(self, T: np.ndarray, Y: np.ndarray) -> np.ndarray:
@@ -157,19 +164,36 @@ def _cd6(f: np.ndarray, axis: int, n: int) -> np.ndarray:
     return 1 / 60 * (s(3) - s(-3)) - 3 / 20 * (s(2) - s(-2)) + 3 / 4 * (s(1) - s(-1))
 
 
-def metrics_from_mapping(xyz, nx: int, ny: int, nz: int) -> dict[str, np.ndarray]:
+def _sin(x):
+    """np.sin for numpy arrays, torch.sin for torch tensors (the mappings serve both)."""
+    return np.sin(x) if isinstance(x, (np.ndarray, float)) else x.sin()
+
+
+def _array_ops(device):
+    """(arange, meshgrid, zeros) in float64: numpy when `device` is None, else torch on it."""
+    if device is None:
+        return (lambda a, b: np.arange(a, b, dtype=np.float64), np.meshgrid,
+                lambda s: np.zeros(s))
+    import torch
+    return (lambda a, b: torch.arange(a, b, dtype=torch.float64, device=device), torch.meshgrid,
+            lambda s: torch.zeros(s, dtype=torch.float64, device=device))
+
+
+def metrics_from_mapping(xyz, nx: int, ny: int, nz: int, device=None) -> dict:
     """Metrics of a periodic-in-index mapping; xyz(i, j, k) -> (x, y, z) for index arrays.
 
-    Returns the ten ghosted (Tz, Ty, Tx) arrays named as in FlameMetrics."""
+    Returns the ten ghosted (Tz, Ty, Tx) arrays named as in FlameMetrics: numpy arrays, or
+    torch tensors built on `device` when one is given (same operations in the same order)."""
+    arange, meshgrid, zeros = _array_ops(device)
     e = 3
     der = {}
     for ax, n in enumerate((nx, ny, nz)):
         # coordinates extended by 3 along this axis only, interior along the other two
-        ii = np.arange(-e, nx + e) if ax == 0 else np.arange(nx)
-        jj = np.arange(-e, ny + e) if ax == 1 else np.arange(ny)
-        kk = np.arange(-e, nz + e) if ax == 2 else np.arange(nz)
-        K, J, I = np.meshgrid(kk, jj, ii, indexing="ij")
-        X, Y, Z = xyz(I.astype(np.float64), J.astype(np.float64), K.astype(np.float64))
+        ii = arange(-e, nx + e) if ax == 0 else arange(0, nx)
+        jj = arange(-e, ny + e) if ax == 1 else arange(0, ny)
+        kk = arange(-e, nz + e) if ax == 2 else arange(0, nz)
+        K, J, I = meshgrid(kk, jj, ii, indexing="ij")
+        X, Y, Z = xyz(I, J, K)
         npax = 2 - ax  # numpy axis of i/j/k
         der["x", ax] = _cd6(X, npax, n)
         der["y", ax] = _cd6(Y, npax, n)
@@ -193,30 +217,37 @@ def metrics_from_mapping(xyz, nx: int, ny: int, nz: int) -> dict[str, np.ndarray
         "dzetadz": dxdxi * dydeta - dxdeta * dydxi,
         "J": Jm,
     }
+    del der, dxdxi, dxdeta, dxdzeta, dydxi, dydeta, dydzeta, dzdxi, dzdeta, dzdzeta
     tx, ty, tz = ghosted(nx, ny, nz)
     out = {}
     for k in METRIC_NAMES:
-        a = np.zeros((1, tz, ty, tx))
-        a[0, NG:NG + nz, NG:NG + ny, NG:NG + nx] = vals[k]
+        a = zeros((1, tz, ty, tx))
+        a[0, NG:NG + nz, NG:NG + ny, NG:NG + nx] = vals.pop(k)
         periodic_fill(a, nx, ny, nz)
         out[k] = a[0]
     return out
 
 
-def cartesian_metrics(nx, ny, nz, hx, hy, hz):
-    return metrics_from_mapping(lambda i, j, k: (i * hx, j * hy, k * hz), nx, ny, nz)
+def cartesian_metrics(nx, ny, nz, hx, hy, hz, device=None):
+    return metrics_from_mapping(lambda i, j, k: (i * hx, j * hy, k * hz), nx, ny, nz, device)
 
 
-def wavy_metrics(nx, ny, nz, amp=0.1):
-    """x = ξ + a sin2πη sin2πζ, y = η + a sin2πζ sin2πξ, z = ζ + a sin2πξ sin2πη with
-    ξ = i/nx, η = j/ny, ζ = k/nz (the curvilinear benchmark mapping)."""
+def wavy_mapping(nx, ny, nz, amp=0.1, scale=1.0):
+    """x = s (ξ + a sin2πη sin2πζ), y = s (η + a sin2πζ sin2πξ), z = s (ζ + a sin2πξ sin2πη)
+    with ξ = i/nx, η = j/ny, ζ = k/nz (the curvilinear benchmark mapping, scaled by s)."""
     tp = 2 * math.pi
 
     def xyz(i, j, k):
         xi, eta, zeta = i / nx, j / ny, k / nz
-        return (xi + amp * np.sin(tp * eta) * np.sin(tp * zeta),
-                eta + amp * np.sin(tp * zeta) * np.sin(tp * xi),
-                zeta + amp * np.sin(tp * xi) * np.sin(tp * eta))
+        x = xi + amp * _sin(tp * eta) * _sin(tp * zeta)
+        y = eta + amp * _sin(tp * zeta) * _sin(tp * xi)
+        z = zeta + amp * _sin(tp * xi) * _sin(tp * eta)
+        return (x, y, z) if scale == 1.0 else (scale * x, scale * y, scale * z)
+    return xyz
+
+
+def wavy_metrics(nx, ny, nz, amp=0.1):
+    xyz = wavy_mapping(nx, ny, nz, amp)
     return metrics_from_mapping(xyz, nx, ny, nz), xyz
 
 

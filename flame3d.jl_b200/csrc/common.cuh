@@ -222,6 +222,25 @@ __device__ __forceinline__ T wenoz_combine_fast(T s11_, T s22_, T s33_, T v1, T 
     return T((a1 * double(v1) + a2 * double(v2) + a3 * double(v3)) / (6.0 * (a1 + a2 + a3)));
 }
 
+// FP32 form for the mixed-precision paths, in the reference's own shape α_k = d_k (1 + q_k²),
+// q_k = τ / (ε + β_k), with every step kept inside FP32 range: q_k is capped at 1e15 (a stencil
+// with q_k that large already carries weight 1 to FP32 precision; when two are capped their
+// candidate values agree to far below FP32 resolution, since β_k < 1e-15 τ bounds their second
+// differences), the α_k are normalised by their sum before they multiply the candidates, and
+// the divisions are the fast approximate ones (2 ulp), ample for weights in FP32.
+template <>
+__device__ __forceinline__ float wenoz_combine_fast<float>(float s11, float s22, float s33,
+                                                           float v1, float v2, float v3) {
+    constexpr float eps = float(kWenoEps), qmax = 1e15f;
+    const float tau = fabsf(s11 - s33);
+    const float q1 = fminf(__fdividef(tau, eps + s11), qmax);
+    const float q2 = fminf(__fdividef(tau, eps + s22), qmax);
+    const float q3 = fminf(__fdividef(tau, eps + s33), qmax);
+    const float a1 = 1.0f + q1 * q1, a2 = 6.0f * (1.0f + q2 * q2), a3 = 3.0f * (1.0f + q3 * q3);
+    const float r = __fdividef(1.0f, a1 + a2 + a3);
+    return (1.0f / 6.0f) * ((a1 * r) * v1 + (a2 * r) * v2 + (a3 * r) * v3);
+}
+
 template <typename T>
 __device__ __forceinline__ T wenoz_plus_fast(T V1, T V2, T V3, T V4, T V5) {
     const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);

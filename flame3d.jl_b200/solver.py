@@ -48,6 +48,8 @@ class DeviceCase:
         qdt = torch.float64 if precision == 0 else torch.float32
 
         def up(a, dtype=torch.float64):
+            if isinstance(a, torch.Tensor):  # built on the device: adopted when dtype matches
+                return a.to(device=dev, dtype=dtype).contiguous()
             return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dtype)
 
         self.metrics = {k: up(case.metrics[k]) for k in METRIC_NAMES}
@@ -66,6 +68,8 @@ class DeviceCase:
         self.T = [torch.empty((3,) + shp, dtype=qdt, device=dev) for _ in range(2)]
         if precision == 0:
             self._call("flame_prim2c", _p(self.U), _p(self.Q[0]))
+        elif isinstance(case.Q, torch.Tensor):  # U from the FP64 primitives, before rounding
+            self._call("flame_prim2c", _p(self.U), _p(up(case.Q)))
         else:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
         self._transport()
