@@ -222,7 +222,7 @@ def run_ensemble(args, f3d) -> int:
     def fifo(precision, fused, k):
         tot = 0.0
         for c in cases:
-            dc = S.DeviceCase(c, device=dev, precision=precision, tile=3,
+            dc = S.DeviceCase(c, device=dev, precision=precision, tile="auto" if fused else 3,
                               sequence_buffers=not fused)
             dc.step(fused)
             torch.cuda.synchronize(dev)
@@ -238,11 +238,12 @@ def run_ensemble(args, f3d) -> int:
 
     plain, plain_ms = fifo(0, True, 3)
     seq, seq_ms = fifo(0, False, 1)
-    dcs = [S.DeviceCase(c, device=dev, precision=1, tile=3) for c in cases]
+    pencil = [S.DeviceCase(c, device=dev, precision=1, tile=3) for c in cases]
+    tuned = [S.DeviceCase(c, device=dev, precision=1, tile="auto") for c in cases]
     k = max(args.steps // 10, 10)
     modes = {}
-    for mode in ("graph", "persistent"):
-        batch = B.Batch(dcs, device=dev, mode=mode)
+    for mode, dcs in (("graph", tuned), ("graph_pencil", pencil), ("persistent", pencil)):
+        batch = B.Batch(dcs, device=dev, mode=mode.split("_")[0])
         batch.capture()
         for _ in range(max(args.warmup, 3)):
             batch.step()
@@ -264,9 +265,15 @@ def run_ensemble(args, f3d) -> int:
            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
            "data": "synthetic (seeded Taylor-Green ensemble with Fourier perturbations)",
            "config": {"workload": "ensemble64", "cases": len(cases), "cells": cells,
-                      "path": f"batched pencil sweeps ({best} mode), mixed precision, CUDA graph per step",
+                      "path": f"batched stages ({best} mode), mixed precision, CUDA graph per step",
                       "modes": {m: v[0] for m, v in modes.items()},
-                      "launches_per_step": 3 * 4 * len({c.ns for c in cases})},
+                      "tuned_configs": {str(t): sum(d.tile == t for d in tuned)
+                                        for t in sorted({d.tile for d in tuned})},
+                      "launches_per_step": (3 * sum(d.launches_per_stage() for d in tuned)
+                                            if best == "graph" else
+                                            3 * sum(d.launches_per_stage() for d in pencil)
+                                            if best == "graph_pencil" else
+                                            3 * 4 * len({c.ns for c in cases}))},
            "step_latency_ms": {"p50": _pct(per_step, 50), "p99": _pct(per_step, 99)},
            "plain_fp64_fused_fifo": {"value": plain, "unit": UNIT, "ms_per_step_all_cases": plain_ms},
            "plain_fp64_launch_sequence_fifo": {"value": seq, "unit": UNIT,
@@ -359,6 +366,9 @@ def run_serve(args, f3d) -> int:
     warm = S.request_stream(3, rate=1000.0, seed=6, n_range=(16, 24), steps_range=(2, 3))
     S.fifo(warm, dev, precision=0)  # module loads, allocator, graph pools
     S.Server(dev, precision=1).run(warm)
+    t_tune = time.perf_counter()
+    tuned = S.pretune(reqs, dev)  # the autotuner's cache for every key of the stream
+    t_tune = time.perf_counter() - t_tune
     torch.cuda.synchronize(dev)
     props = torch.cuda.get_device_properties(dev)
     uuid = getattr(props, "uuid", None)
@@ -387,7 +397,9 @@ def run_serve(args, f3d) -> int:
            "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": 20.0,
                       "seed": 5, "step_scale": args.step_scale, "hbm_budget_bytes": 150e9,
                       "cell_stages": sum(r.cell_stages for r in reqs),
-                      "path": "continuous batching, graph-mode batch, mixed precision",
+                      "path": "continuous batching, graph-mode batch, mixed precision, "
+                              "autotuned stage configurations (both arms)",
+                      "autotune": {"keys_tuned_before_serving": tuned, "seconds": t_tune},
                       "l2": "inputs of the large cases exceed L2; no flush between steps"},
            "step_latency_ms": rep["step_latency_ms"],
            "completion_latency_s": rep["completion_latency_s"],
@@ -408,7 +420,7 @@ def main() -> int:
     ap.add_argument("--workload", default="jet256x128x128", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-stages", type=int, default=3)
-    ap.add_argument("--tile", type=int, default=None,
+    ap.add_argument("--tile", type=lambda v: v if v == "auto" else int(v), default="auto",
                     help="stage configuration (0-3); default: the autotuner's choice")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests in the stream")

@@ -38,9 +38,8 @@ class Batch:
         if len(prec) != 1:
             raise abi.FlameError(1, "all cases of a batch share one precision")
         self.precision = prec.pop()
-        for dc in self.cases:
-            if dc.tile != 3 or dc.scratch is None:
-                raise abi.FlameError(1, "batched cases use the pencil configuration (tile=3)")
+        if mode == "persistent" and any(dc.tile != 3 or dc.scratch is None for dc in self.cases):
+            raise abi.FlameError(1, "the persistent batch runs the pencil configuration (tile=3)")
         self.mode = mode
         self.parity = 0
         self.graphs: dict[int, torch.cuda.CUDAGraph] = {}

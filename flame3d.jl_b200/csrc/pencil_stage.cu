@@ -390,8 +390,11 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
             }
 }
 
-// x sweep (lanes along x, every access coalesced); it is the last sweep and finishes the stage.
-template <int NS, typename QT, typename CT>
+// x sweep (lanes along x, every access coalesced); it is the last sweep.  FIN: it finishes the
+// stage itself (configuration 3); otherwise it adds its differences to R and k_finish follows
+// (configuration 4: the FP64 finish then runs at full occupancy, apart from the sweep's
+// registers and shared memory).  Both round R + rhs once, so they agree bit for bit.
+template <int NS, typename QT, typename CT, bool FIN = true>
 __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned char *smem_raw) {
     constexpr int WPB = Wpb<0>::value;
     using SL = Slots<NS>;
@@ -421,13 +424,32 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
 #pragma unroll
     for (int n = 0; n < 5 + NS; ++n)
         rhs[n] = double(S[(SL::G + n) * 32 + lane]) - double(S[(SL::G + n) * 32 + lane + 1]);
-    finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
+    if constexpr (FIN) {
+        finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
+    } else {
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * A.np] += rhs[n];
+    }
 }
 
-template <int NS, typename QT, typename CT>
+template <int NS, typename QT, typename CT, bool FIN>
 __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    x_block<NS, QT, CT>(A, blockIdx.x, smem_raw);
+    x_block<NS, QT, CT, FIN>(A, blockIdx.x, smem_raw);
+}
+
+// The stage's finish for configuration 4: one thread per interior cell, x fastest, with the
+// complete right-hand side already in R.
+template <int NS, typename QT>
+__global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT> A) {
+    const int c = blockIdx.x * 128 + threadIdx.x;
+    if (c >= A.nx * A.ny * A.nz) return;
+    const int x = c % A.nx, y = (c / A.nx) % A.ny, z = c / (A.nx * A.ny);
+    const int gx = x + A.ng, gy = y + A.ng, gz = z + A.ng;
+    double rhs[5 + NS];
+#pragma unroll
+    for (int n = 0; n < 5 + NS; ++n) rhs[n] = 0.0;
+    finish_cell<NS, QT>(A, gx + A.sy * gy + A.sz * gz, gx, gy, gz, rhs);
 }
 
 // Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
@@ -609,36 +631,40 @@ int launch_staged(const Args<QT> &A, cudaStream_t s) {
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
-template <int NS, typename QT, typename CT>
+template <int NS, typename QT, typename CT, bool FIN>
 int launch_x(const Args<QT> &A, cudaStream_t s) {
     constexpr int WPB = Wpb<0>::value;
     constexpr size_t sm = smem_bytes<NS, CT, WPB>();
     static bool done[64] = {};
-    if (int e = set_smem(k_pencil_x<NS, QT, CT>, sm, done)) return e;
+    if (int e = set_smem(k_pencil_x<NS, QT, CT, FIN>, sm, done)) return e;
     const long long warps = (long long)A.ny * A.nz * ((A.nx + OWN - 1) / OWN);
-    k_pencil_x<NS, QT, CT><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
+    k_pencil_x<NS, QT, CT, FIN><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
 template <int NS, typename QT, typename CT>
 int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const FlameStageBuffers &b,
            const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr,
-           void *scratch) {
+           void *scratch, bool split_finish) {
     const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr, scratch);
     k_prep<NS, QT><<<(unsigned)((A.np + 255) / 256), 256, 0, s>>>(A);
     if (int e = flame_check_launch("flame_rk_stage (prep)")) return e;
     if (int e = launch_staged<2, 0, NS, QT, CT>(A, s)) return e;
     if (int e = launch_staged<1, 1, NS, QT, CT>(A, s)) return e;
-    return launch_x<NS, QT, CT>(A, s);
+    if (!split_finish) return launch_x<NS, QT, CT, true>(A, s);
+    if (int e = launch_x<NS, QT, CT, false>(A, s)) return e;
+    const long long cells = (long long)A.nx * A.ny * A.nz;
+    k_finish<NS, QT><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(A);
+    return flame_check_launch("flame_rk_stage (finish)");
 }
 
 template <typename QT, typename CT>
 int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
              const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
-             const FlameTransport &tr, void *scratch) {
+             const FlameTransport &tr, void *scratch, bool split_finish) {
     switch (ns) {
 #define CASE(N) \
-    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr, scratch);
+    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr, scratch, split_finish);
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
         default:
@@ -653,16 +679,16 @@ int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
 // Entry used by fused_stage.cu's dispatcher for tile configuration 3.
 int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
                        const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *th,
-                       const FlameTransport *tr, int precision, void *scratch) {
+                       const FlameTransport *tr, int precision, void *scratch, int split_finish) {
     if (!scratch)
         return flame_fail(FLAME_EINVAL,
                           "flame_rk_stage: the pencil configuration needs scratch (see "
                           "flame_stage_scratch_bytes)");
     if (precision == 0)
         return flame::pencil::dispatch<double, double>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
-                                                       scratch);
+                                                       scratch, split_finish != 0);
     return flame::pencil::dispatch<float, float>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
-                                                 scratch);
+                                                 scratch, split_finish != 0);
 }
 
 extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {

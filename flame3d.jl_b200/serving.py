@@ -295,7 +295,7 @@ class Server:
     def __init__(self, device="cuda", precision: int = 1, hbm_budget: float = 150e9,
                  max_slots: int = 64, streams: int = 16, capture: bool = True,
                  keep_results: bool = False, builder=build_request_case,
-                 capture_min_steps: int = 8):
+                 capture_min_steps: int = 8, tile="auto"):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise abi.FlameError(1, "the server needs a CUDA device")
@@ -306,6 +306,7 @@ class Server:
         self.streams = streams
         self.capture = capture
         self.capture_min_steps = capture_min_steps
+        self.tile = tile
         self.keep_results = keep_results
         self.builder = builder
         self.results: dict[int, tuple[np.ndarray, np.ndarray]] = {}
@@ -319,7 +320,7 @@ class Server:
         rec.admitted = now
         with torch.cuda.stream(self.build_stream):
             case = self.builder(req, self.device)
-            dc = DeviceCase(case, self.device, precision=self.precision, tile=3)
+            dc = DeviceCase(case, self.device, precision=self.precision, tile=self.tile)
         case.Q = case.rhoi = None  # the DeviceCase holds the state now
         case.metrics = {}
         torch.cuda.current_stream(self.device).wait_stream(self.build_stream)
@@ -502,8 +503,30 @@ def _report(records, step_ms, st) -> dict:
     }
 
 
+def pretune(requests: list[SolveRequest], device="cuda", precisions=(0, 1),
+            builder=build_request_case) -> int:
+    """Fills the autotuner's cache for every (precision, species, size class) the requests
+    need, ahead of serving; returns the number of configurations tuned."""
+    from . import autotune
+    tuner = autotune.default()
+    gpu = tuner.gpu_name(torch.device(device))
+    todo = {}
+    for r in requests:
+        for p in precisions:
+            todo.setdefault(autotune.key(gpu, p, r.ns, r.cells), (r, p))
+    n = 0
+    for k, (r, p) in todo.items():
+        if k in tuner.table:
+            continue
+        dc = DeviceCase(builder(r, device), device, precision=p, tile="auto")
+        del dc
+        n += 1
+    torch.cuda.empty_cache()
+    return n
+
+
 def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
-         keep_results: bool = False, builder=build_request_case) -> dict:
+         keep_results: bool = False, builder=build_request_case, tile="auto") -> dict:
     """The baseline: one case at a time in arrival order (plain stage launches, no batching,
     no graphs), same arrival times, same GPU, same report."""
     dev = torch.device(device)
@@ -522,7 +545,7 @@ def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
         rec.admitted = now()
         tb = time.perf_counter()
         case = builder(r, dev)
-        dc = DeviceCase(case, dev, precision=precision, tile=3)
+        dc = DeviceCase(case, dev, precision=precision, tile=tile)
         case.Q = case.rhoi = None
         case.metrics = {}
         rec.name = case.name

@@ -73,14 +73,42 @@ class DeviceCase:
         else:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
         self._transport()
-        self.tile = 3 if tile is None else tile  # the pencil sweeps: fastest on every case measured
         self.scratch = None
-        if self.tile == 3:
-            nbytes = self.lib.flame_stage_scratch_bytes(C.byref(self.grid), precision)
-            self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         self.seq = None
+        # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice, or
+        # None for the pencil sweeps (configuration 3)
+        self.set_tile(3 if tile is None or tile == "auto" else tile)
+        if tile == "auto":
+            from . import autotune
+            self.set_tile(autotune.default().choose(self))
         if sequence_buffers:
             self._alloc_sequence()
+
+    def set_tile(self, tile: int) -> None:
+        """Switches the fused stage's configuration (the pencil ones need scratch)."""
+        self.tile = int(tile)
+        if self.tile in (3, 4):
+            if self.scratch is None:
+                nbytes = self.lib.flame_stage_scratch_bytes(C.byref(self.grid), self.precision)
+                self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        else:
+            self.scratch = None
+
+    def clone(self, tile: int | None = None) -> "DeviceCase":
+        """A copy of the current state on the same device (metrics shared: no kernel writes
+        them), optionally with another configuration."""
+        c = DeviceCase.__new__(DeviceCase)
+        for a in ("lib", "case", "device", "precision", "grid", "thermo", "transport", "dt",
+                  "metrics", "cmetrics", "cur"):
+            setattr(c, a, getattr(self, a))
+        c.Q = [q.clone() for q in self.Q]
+        c.rhoi = [r.clone() for r in self.rhoi]
+        c.T = [t.clone() for t in self.T]
+        c.U, c.Un, c.rhon = self.U.clone(), self.Un.clone(), self.rhon.clone()
+        c.scratch = None
+        c.seq = None
+        c.set_tile(self.tile if tile is None else tile)
+        return c
 
     # ------------------------------------------------------------------ plumbing
     @property
@@ -163,12 +191,16 @@ class DeviceCase:
         self.cur = o
 
     def launches_per_stage(self) -> int:
-        """Kernels one fused stage launches: 4 for the pencil sweeps, 1 for a tile kernel."""
-        return 4 if self.tile == 3 else 1
+        """Kernels one fused stage launches: 4 (5 with the separate finish) for the pencil
+        sweeps, 1 for a tile kernel."""
+        return {3: 4, 4: 5}.get(self.tile, 1)
 
     def stage_kernels(self) -> str:
         if self.tile == 3:
             return "pencil::k_prep + k_pencil_staged<z> + k_pencil_staged<y> + k_pencil_x"
+        if self.tile == 4:
+            return ("pencil::k_prep + k_pencil_staged<z> + k_pencil_staged<y> + k_pencil_x"
+                    " + k_finish")
         return "fused::k_stage<tile %d>" % self.tile
 
     def step(self, fused: bool = True) -> None:

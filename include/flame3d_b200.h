@@ -201,22 +201,24 @@ typedef struct FlameStageBuffers {
     double *rhon;          /* (…,ns) RK3 stage-0 copy */
     const void *trans_in;  /* (…,3) μ, λ, D of the stage input */
     void *trans_out;       /* (…,3) μ, λ, D of the stage result */
-    void *scratch;         /* flame_stage_scratch_bytes() bytes for tile configuration 3, else
-                              unused (may be NULL); contents need not survive between calls */
+    void *scratch;         /* flame_stage_scratch_bytes() bytes for configurations 3 and 4,
+                              else unused (may be NULL); contents need not survive calls */
 } FlameStageBuffers;
 
 /* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 storage of Q and transport, FP32
- * split / reconstruction / viscous fluxes; FP64 conserved accumulation, metrics, WENO-Z weights
- * and Newton temperature).  No reference counterpart: it replaces the launch sequence of
- * solver.jl:298-326. */
+ * split / reconstruction with its WENO-Z weights / viscous fluxes; FP64 conserved accumulation,
+ * metrics and Newton temperature).  No reference counterpart: it replaces the launch sequence
+ * of solver.jl:298-326. */
 int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                    const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *thermo,
                    const FlameTransport *transport, int precision);
 
 /* flame_rk_stage with an explicit configuration: 0, 1, 2 = one tile kernel per stage (16x8x8
  * with one CTA per SM, 16x8x8 with two, 8x8x8 with two); 3 = four barrier-free launches
- * (a prep pass and z, y, x warp-per-pencil sweeps) that need b->scratch.  The autotuner picks
- * the configuration per grid, species count and precision. */
+ * (a prep pass and z, y, x warp-per-pencil sweeps, the x sweep finishing the stage) that need
+ * b->scratch; 4 = configuration 3 with the finish (RK3 update, c2Prim, transport, ghosts) in a
+ * fifth, per-cell launch, bit-identical to 3.  The autotuner picks the configuration per grid,
+ * species count and precision. */
 int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                          const FlameStageBuffers *b, const FlameMetrics *m,
                          const FlameThermo *thermo, const FlameTransport *transport,

@@ -63,7 +63,7 @@ def test_sequence_matches_oracle(f3d, oracle, cuda_ok, name):
     assert max(e.values()) <= 1e-14, e
 
 
-TILES = [0, 1, 2, 3]
+TILES = [0, 1, 2, 3, 4]
 
 
 @pytest.mark.parametrize("tile", TILES)
@@ -116,3 +116,37 @@ def test_fused_mixed_precision_error(f3d, oracle, cuda_ok, name, tile):
     e = _errors(dc, oc, oracle)
     for f in ("rho", "rhou", "E"):
         assert e[f] <= 1e-5, (f, e)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_split_finish_is_bit_identical(f3d, cuda_ok, precision):
+    """Configuration 4 (finish in its own launch) rounds R + rhs once, like configuration 3."""
+    S = f3d.solver_module()
+    case = f3d.random_curvilinear(n=12, ns=3, seed=61)
+    a = S.DeviceCase(case, precision=precision, tile=3)
+    b = a.clone(tile=4)
+    for _ in range(2):
+        a.step()
+        b.step()
+    for x, y in zip(a.primitives() + (a.conserved(),), b.primitives() + (b.conserved(),)):
+        assert np.array_equal(x, y)
+
+
+def test_autotuned_case_matches_fixed_configuration(f3d, cuda_ok, tmp_path, monkeypatch):
+    monkeypatch.setenv("FLAME3D_B200_CACHE", str(tmp_path))
+    S = f3d.solver_module()
+    import importlib
+    A = importlib.import_module(f3d.__name__ + ".autotune")
+    monkeypatch.setattr(A, "_DEFAULT", None)
+    case = f3d.random_curvilinear(n=12, ns=2, seed=62)
+    auto = S.DeviceCase(case, tile="auto")
+    assert auto.tile in A.CANDIDATES
+    assert (tmp_path / "autotune.json").exists()
+    fixed = S.DeviceCase(case, tile=3)
+    auto.step()
+    fixed.step()
+    Ua, Uf = auto.conserved(), fixed.conserved()
+    mom = np.linalg.norm(Uf[1:4].ravel())
+    for n in range(5):
+        scale = mom if 1 <= n <= 3 else np.linalg.norm(Uf[n].ravel())
+        assert np.linalg.norm((Ua[n] - Uf[n]).ravel()) <= 1e-12 * scale
