@@ -51,6 +51,11 @@ METRIC_NAMES = ("dxidx", "dxidy", "dxidz", "detadx", "detady", "detadz",
                 "dzetadx", "dzetady", "dzetadz", "J")
 
 
+class FlameInflow(C.Structure):
+    _fields_ = [("P", C.c_double), ("T", C.c_double), ("u", C.c_double), ("v", C.c_double),
+                ("w", C.c_double), ("Y", C.c_double * FLAME_MAX_NS)]
+
+
 class FlameMetrics(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in METRIC_NAMES]
 
@@ -95,6 +100,14 @@ SIGNATURES = {
     "flame_prim2c": [G, S, P, P],
     "flame_mixture": [G, S, P, P, P, P, P, P, TH, TR, P],
     "flame_fill_periodic": [G, S, P, I],
+    "flame_fill_x": [G, S, P, P, P, P, TH, C.POINTER(FlameInflow), I, I],
+    "flame_fill_y": [G, S, P, P],
+    "flame_fill_z": [G, S, P, P, P, P, TH, C.POINTER(FlameInflow)],
+    "flame_fill_y_s": [G, S, P],
+    "flame_fill_z_s": [G, S, P],
+    "flame_fillGhost": [G, S, P, P, P, P, TH, C.POINTER(FlameInflow), I, I],
+    "flame_fillSpec": [G, S, P],
+    "flame_cfl_max": [G, S, P, M, P],
     "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
     "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],

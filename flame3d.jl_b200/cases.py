@@ -142,6 +142,19 @@ def ghosted(nx: int, ny: int, nz: int) -> tuple[int, int, int]:
     return nx + 2 * NG, ny + 2 * NG, nz + 2 * NG
 
 
+def reference_inflow(ns: int):
+    """The inflow state fill_x / fill_z hard-code (boundary.jl:17-25, 96-104): P = 79.8 Pa,
+    T = 270.65 K, u = 1000 m/s, v = w = 0, Y(2) = 0.233 and Y(5) = 0.767 (1-based species
+    indices, so ns >= 5), every other mass fraction zero."""
+    from .abi import FlameInflow
+    if ns < 5:
+        raise ValueError("the reference inflow sets species 2 and 5: ns >= 5")
+    f = FlameInflow()
+    f.P, f.T, f.u, f.v, f.w = 79.8, 270.65, 1000.0, 0.0, 0.0
+    f.Y[1], f.Y[4] = 0.233, 0.767
+    return f
+
+
 def periodic_fill(a: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     """Copies every ghost of a (nv, Tz, Ty, Tx) array from its periodic image, in place
     (axis by axis, so edges and corners come from the images already filled)."""

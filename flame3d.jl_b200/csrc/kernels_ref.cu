@@ -415,6 +415,116 @@ __global__ void k_fill_periodic(Dims D, double *__restrict__ A, int nv, int peri
     for (int n = 0; n < nv; ++n) A[dst + n * D.np] = A[src + n * D.np];
 }
 
+// ------------------------------------------------------------------ boundary.jl:1-176
+// The inflow state of fill_x / fill_z (boundary.jl:10-43, 89-122): every Yi and ρi zeroed, the
+// inflow's Y set, ρ = ρmixture(P, T, Y) (thermo.jl:29-35), ρi = Y ρ, e = InternalEnergy(T, ρi),
+// then Q and U.
+__device__ void set_inflow(const Dims &D, long long p, double *Q, double *U, double *rhoi,
+                           double *Yi, const FlameThermo &th, const FlameInflow &in) {
+    const int ns = D.ns;
+    const long long np = D.np;
+    for (int n = 0; n < ns; ++n) Yi[p + n * np] = 0.0, rhoi[p + n * np] = 0.0;
+    for (int n = 0; n < ns; ++n) Yi[p + n * np] = in.Y[n];
+    double yow = 0;
+    for (int n = 0; n < ns; ++n) yow += Yi[p + n * np] / th.mw[n];
+    const double rho = in.P / (th.Ru * in.T * yow);
+    double r[FLAME_MAX_NS];
+    for (int n = 0; n < ns; ++n) {
+        rhoi[p + n * np] = Yi[p + n * np] * rho;
+        r[n] = rhoi[p + n * np];
+    }
+    const double ei = internal_energy<0>(th, ns, in.T, r);
+    const double u = in.u, v = in.v, w = in.w;
+    const double q[7] = {rho, u, v, w, in.P, in.T, ei};
+    for (int n = 0; n < 7; ++n) Q[p + n * np] = q[n];
+    U[p] = rho;
+    U[p + np] = u * rho;
+    U[p + 2 * np] = v * rho;
+    U[p + 3 * np] = w * rho;
+    U[p + 4 * np] = ei + 0.5 * rho * (u * u + v * v + w * w);
+}
+
+__device__ void copy_point(const Dims &D, long long dst, long long src, double *Q, double *U,
+                           double *rhoi) {
+    for (int n = 0; n < 7 && Q; ++n) Q[dst + n * D.np] = Q[src + n * D.np];
+    for (int n = 0; n < 5 && U; ++n) U[dst + n * D.np] = U[src + n * D.np];
+    for (int n = 0; n < D.ns && rhoi; ++n) rhoi[dst + n * D.np] = rhoi[src + n * D.np];
+}
+
+// fill_x, boundary.jl:1-52 (0-based: inflow i <= NG, outlet i >= nx+NG-1 from nx+NG-2)
+__global__ void k_fill_x(Dims D, double *Q, double *U, double *rhoi, double *Yi, FlameThermo th,
+                         FlameInflow in, int rank, int nprocs) {
+    long long i = blockIdx.x * (long long)BX + threadIdx.x;
+    long long j = blockIdx.y * (long long)BY + threadIdx.y;
+    long long k = blockIdx.z * (long long)BZ + threadIdx.z;
+    if (i >= D.tx || j >= D.ty || k >= D.tz) return;
+    const long long p = D.P(i, j, k);
+    if (rank == 0 && i <= D.ng) set_inflow(D, p, Q, U, rhoi, Yi, th, in);
+    if (rank == nprocs - 1 && i >= D.nx + D.ng - 1)
+        copy_point(D, p, D.P(D.nx + D.ng - 2, j, k), Q, U, rhoi);
+}
+
+// fill_y (boundary.jl:54-80) on Q, U and fill_y_s (139-158) on ρi: the same rule
+__global__ void k_fill_y(Dims D, double *Q, double *U, double *rhoi) {
+    long long i = blockIdx.x * (long long)BX + threadIdx.x;
+    long long j = blockIdx.y * (long long)BY + threadIdx.y;
+    long long k = blockIdx.z * (long long)BZ + threadIdx.z;
+    if (i >= D.tx || j >= D.ty || k >= D.tz) return;
+    if (j <= D.ng)
+        copy_point(D, D.P(i, j, k), D.P(i, D.ng + 1, k), Q, U, rhoi);
+    else if (j >= D.ny + D.ng - 1)
+        copy_point(D, D.P(i, j, k), D.P(i, D.ny + D.ng - 2, k), Q, U, rhoi);
+}
+
+// fill_z (boundary.jl:82-137): inflow k <= NG, outlet k >= nz+NG-1 copies Q, U only;
+// fill_z_s (160-176) with Q = U = null: the outlet copy of ρi
+__global__ void k_fill_z(Dims D, double *Q, double *U, double *rhoi, double *Yi, FlameThermo th,
+                         FlameInflow in, int inflow) {
+    long long i = blockIdx.x * (long long)BX + threadIdx.x;
+    long long j = blockIdx.y * (long long)BY + threadIdx.y;
+    long long k = blockIdx.z * (long long)BZ + threadIdx.z;
+    if (i >= D.tx || j >= D.ty || k >= D.tz) return;
+    const long long p = D.P(i, j, k);
+    if (inflow && k <= D.ng)
+        set_inflow(D, p, Q, U, rhoi, Yi, th, in);
+    else if (k >= D.nz + D.ng - 1)
+        copy_point(D, p, D.P(i, j, D.nz + D.ng - 2), Q, U, inflow ? nullptr : rhoi);
+}
+
+// CFL rate of every interior cell, reduced to its maximum (see flame_cfl_max).  A non-negative
+// double orders like its bit pattern read as an unsigned integer, so an integer atomicMax of
+// the bits is the exact maximum in any order (a NaN rate sorts above every number and so
+// propagates).
+__global__ void k_cfl_max(Dims D, const double *__restrict__ Q, FlameMetrics m,
+                          unsigned long long *out) {
+    const long long c = blockIdx.x * 256LL + threadIdx.x;
+    const long long ncell = (long long)D.nx * D.ny * D.nz;
+    unsigned long long bits = 0;
+    if (c < ncell) {
+        const long long x = c % D.nx, y = (c / D.nx) % D.ny, z = c / ((long long)D.nx * D.ny);
+        const long long p = D.P(x + D.ng, y + D.ng, z + D.ng), np = D.np;
+        const double rho = Q[p], u = Q[p + np], v = Q[p + 2 * np], w = Q[p + 3 * np],
+                     pr = Q[p + 4 * np], e = Q[p + 6 * np];
+        const double gam = pr / e + 1;
+        const double cs = sqrt(gam * pr / rho);
+        const double J = m.J[p];
+        const double *rows[3][3] = {{m.dxidx, m.dxidy, m.dxidz},
+                                    {m.detadx, m.detady, m.detadz},
+                                    {m.dzetadx, m.dzetady, m.dzetadz}};
+        double tot = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double mx = rows[d][0][p], my = rows[d][1][p], mz = rows[d][2][p];
+            tot += J * (fabs(mx * u + my * v + mz * w) + cs * sqrt(mx * mx + my * my + mz * mz));
+        }
+        bits = (unsigned long long)__double_as_longlong(tot);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long b = __shfl_down_sync(0xffffffffu, bits, o);
+        bits = b > bits ? b : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits) atomicMax(out, bits);
+}
+
 }  // namespace
 }  // namespace flame
 
@@ -600,6 +710,91 @@ int flame_mixture(const FlameGrid *g, flame_stream_t s, const double *Q, const d
     k_mixture<<<(unsigned)((D.np + 255) / 256), 256, 0, s>>>(D, Q, rhoi, Yi, lambda, mu, Dk, *th,
                                                               *tr, tag);
     return flame_check_launch("flame_mixture");
+}
+
+static int check_fill_grid(const FlameGrid *g, const char *what) {
+    if (int e = flame_check_grid(g, what)) return e;
+    if (g->nx < 3 || g->ny < 3 || g->nz < 3)
+        return flame_fail(FLAME_EINVAL, "%s: the reference fills need at least 3 cells per axis",
+                          what);
+    return FLAME_OK;
+}
+
+int flame_fill_x(const FlameGrid *g, flame_stream_t s, double *Q, double *U, double *rhoi,
+                 double *Yi, const FlameThermo *th, const FlameInflow *in, int rank, int nprocs) {
+    if (int e = check_fill_grid(g, "flame_fill_x")) return e;
+    if (!Q || !U || !rhoi || !Yi || !th || !in || nprocs < 1 || rank < 0 || rank >= nprocs)
+        return flame_fail(FLAME_EINVAL, "flame_fill_x: NULL argument or bad rank/nprocs");
+    const Dims D = make_dims(*g);
+    k_fill_x<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, Q, U, rhoi, Yi, *th, *in, rank,
+                                                           nprocs);
+    return flame_check_launch("flame_fill_x");
+}
+
+int flame_fill_y(const FlameGrid *g, flame_stream_t s, double *Q, double *U) {
+    if (int e = check_fill_grid(g, "flame_fill_y")) return e;
+    if (!Q || !U) return flame_fail(FLAME_EINVAL, "flame_fill_y: NULL argument");
+    const Dims D = make_dims(*g);
+    k_fill_y<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, Q, U, nullptr);
+    return flame_check_launch("flame_fill_y");
+}
+
+int flame_fill_z(const FlameGrid *g, flame_stream_t s, double *Q, double *U, double *rhoi,
+                 double *Yi, const FlameThermo *th, const FlameInflow *in) {
+    if (int e = check_fill_grid(g, "flame_fill_z")) return e;
+    if (!Q || !U || !rhoi || !Yi || !th || !in)
+        return flame_fail(FLAME_EINVAL, "flame_fill_z: NULL argument");
+    const Dims D = make_dims(*g);
+    k_fill_z<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, Q, U, rhoi, Yi, *th, *in, 1);
+    return flame_check_launch("flame_fill_z");
+}
+
+int flame_fill_y_s(const FlameGrid *g, flame_stream_t s, double *rhoi) {
+    if (int e = check_fill_grid(g, "flame_fill_y_s")) return e;
+    if (!rhoi) return flame_fail(FLAME_EINVAL, "flame_fill_y_s: NULL argument");
+    const Dims D = make_dims(*g);
+    k_fill_y<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, nullptr, nullptr, rhoi);
+    return flame_check_launch("flame_fill_y_s");
+}
+
+int flame_fill_z_s(const FlameGrid *g, flame_stream_t s, double *rhoi) {
+    if (int e = check_fill_grid(g, "flame_fill_z_s")) return e;
+    if (!rhoi) return flame_fail(FLAME_EINVAL, "flame_fill_z_s: NULL argument");
+    const Dims D = make_dims(*g);
+    const FlameThermo th{};
+    const FlameInflow in{};
+    k_fill_z<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, nullptr, nullptr, rhoi, nullptr,
+                                                           th, in, 0);
+    return flame_check_launch("flame_fill_z_s");
+}
+
+int flame_fillGhost(const FlameGrid *g, flame_stream_t s, double *Q, double *U, double *rhoi,
+                    double *Yi, const FlameThermo *th, const FlameInflow *in, int rank,
+                    int nprocs) {
+    if (int e = flame_fill_x(g, s, Q, U, rhoi, Yi, th, in, rank, nprocs)) return e;
+    if (int e = flame_fill_y(g, s, Q, U)) return e;
+    return flame_fill_z(g, s, Q, U, rhoi, Yi, th, in);
+}
+
+int flame_fillSpec(const FlameGrid *g, flame_stream_t s, double *rhoi) {
+    if (int e = flame_fill_y_s(g, s, rhoi)) return e;
+    return flame_fill_z_s(g, s, rhoi);
+}
+
+int flame_cfl_max(const FlameGrid *g, flame_stream_t s, const double *Q, const FlameMetrics *m,
+                  double *out) {
+    if (int e = flame_check_grid(g, "flame_cfl_max")) return e;
+    if (!Q || !m || !out || !m->J || !m->dxidx || !m->dxidy || !m->dxidz || !m->detadx ||
+        !m->detady || !m->detadz || !m->dzetadx || !m->dzetady || !m->dzetadz)
+        return flame_fail(FLAME_EINVAL, "flame_cfl_max: NULL argument");
+    const Dims D = make_dims(*g);
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (e != cudaSuccess)
+        return flame_fail(FLAME_ELAUNCH, "flame_cfl_max: %s", cudaGetErrorString(e));
+    const long long ncell = (long long)D.nx * D.ny * D.nz;
+    k_cfl_max<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(
+        D, Q, *m, reinterpret_cast<unsigned long long *>(out));
+    return flame_check_launch("flame_cfl_max");
 }
 
 int flame_fill_periodic(const FlameGrid *g, flame_stream_t s, double *A, int nv) {

@@ -106,7 +106,18 @@ def _noise_axis(rng, x, kmax=8, nmodes=24):
 
 
 def _cfl_dt(Q, metrics, n, cfl):
-    """cases.cfl_dt with torch operations."""
+    """cases.cfl_dt on the device: flame_cfl_max (strict IEEE, the host rule's operation order)
+    for CUDA tensors, torch operations otherwise."""
+    if Q.is_cuda:
+        import ctypes as C
+        lib = abi.load_library()
+        out = torch.empty(1, dtype=torch.float64, device=Q.device)
+        cm = abi.FlameMetrics(**{k: v.data_ptr() for k, v in metrics.items()})
+        g = abi.FlameGrid(n, n, n, NG, 1, 7)
+        rc = lib.flame_cfl_max(C.byref(g), C.c_void_p(torch.cuda.current_stream(Q.device).cuda_stream),
+                               Q.data_ptr(), C.byref(cm), out.data_ptr())
+        abi.check(lib, rc)
+        return float(cfl / out.item())
     sl = (slice(NG, NG + n),) * 3
     rho, u, v, w, p, e = (Q[k][sl] for k in (0, 1, 2, 3, 4, 6))
     c = torch.sqrt((p / e + 1) * p / rho)

@@ -165,6 +165,51 @@ int flame_mixture(const FlameGrid *g, flame_stream_t stream, const double *Q, co
  * are case-specific inflow / zero-gradient; all benchmark cases are periodic). */
 int flame_fill_periodic(const FlameGrid *g, flame_stream_t stream, double *A, int nv);
 
+/* The inflow state of the reference's fills.  fill_x / fill_z hard-code it (boundary.jl:17-25,
+ * 96-104): P = 79.8 Pa, T = 270.65 K, u = 1000 m/s, v = w = 0, Y(2) = 0.233, Y(5) = 0.767
+ * (1-based species), every other Y zero; here the caller passes it. */
+typedef struct FlameInflow {
+    double P, T, u, v, w;
+    double Y[FLAME_MAX_NS];
+} FlameInflow;
+
+/* boundary.jl:1-52  fill_x(Q, U, ρi, Yi, thermo, rank): on the first x-slab rank the planes
+ * i <= NG+1 (1-based; the first interior plane included) take the inflow state (ρ from
+ * ρmixture, thermo.jl:29-35; e from InternalEnergy), on the last rank the planes i >= Nxp+NG
+ * copy Q, U, ρi from i = Nxp+NG-1.  One GPU: rank 0 of nprocs 1. */
+int flame_fill_x(const FlameGrid *g, flame_stream_t stream, double *Q, double *U, double *rhoi,
+                 double *Yi, const FlameThermo *thermo, const FlameInflow *inflow, int rank,
+                 int nprocs);
+
+/* boundary.jl:54-80  fill_y(Q, U): j <= NG+1 copy j = NG+2, j >= Ny+NG copy j = Ny+NG-1. */
+int flame_fill_y(const FlameGrid *g, flame_stream_t stream, double *Q, double *U);
+
+/* boundary.jl:82-137  fill_z(Q, U, ρi, Yi, thermo): k <= NG+1 inflow (as fill_x), k >= Nz+NG
+ * copy Q, U from k = Nz+NG-1. */
+int flame_fill_z(const FlameGrid *g, flame_stream_t stream, double *Q, double *U, double *rhoi,
+                 double *Yi, const FlameThermo *thermo, const FlameInflow *inflow);
+
+/* boundary.jl:139-158  fill_y_s(ρi): the fill_y rule on ρi. */
+int flame_fill_y_s(const FlameGrid *g, flame_stream_t stream, double *rhoi);
+
+/* boundary.jl:160-176  fill_z_s(ρi): k >= Nz+NG copy k = Nz+NG-1. */
+int flame_fill_z_s(const FlameGrid *g, flame_stream_t stream, double *rhoi);
+
+/* boundary.jl:180-184  fillGhost: fill_x, fill_y, fill_z in that order on the stream. */
+int flame_fillGhost(const FlameGrid *g, flame_stream_t stream, double *Q, double *U,
+                    double *rhoi, double *Yi, const FlameThermo *thermo,
+                    const FlameInflow *inflow, int rank, int nprocs);
+
+/* boundary.jl:188-191  fillSpec: fill_y_s, fill_z_s. */
+int flame_fillSpec(const FlameGrid *g, flame_stream_t stream, double *rhoi);
+
+/* Largest per-cell CFL rate max over interior cells of Σ_d J (|m_d·u| + c |m_d|), with m_d the
+ * stored metric rows (dξ/dx … scaled by 1/J), c = sqrt(γ p / ρ) and γ = p/e + 1 (split.jl:40-41),
+ * written to the device double *out (a stable time step is dt = CFL / *out).  New: the reference
+ * runs a fixed dt (run.jl:30).  Deterministic: the maximum does not depend on reduction order. */
+int flame_cfl_max(const FlameGrid *g, flame_stream_t stream, const double *Q,
+                  const FlameMetrics *m, double *out);
+
 /* solver.jl:22-38  flowAdvance(…): fluxSplit+WENO per direction, viscousFlux ×3, div.
  * Fp/Fm are ghosted (…,5) scratch; Fx/Fy/Fz face (…,5); Fv_* face (…,4); Fh* face (…,3). */
 int flame_flowAdvance(const FlameGrid *g, flame_stream_t stream, double *U, const double *Q,

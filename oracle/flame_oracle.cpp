@@ -675,6 +675,120 @@ void oracle_fill_periodic(const FlameGrid *g, double *A, int nv) {
     }
 }
 
+// ---------------------------------------------------------------- boundary.jl:1-176 fills
+// Reference 1-based planes map to 0-based ones: inflow i <= NG+1 -> i <= NG; outlet
+// i >= Nxp+NG copying Nxp+NG-1 -> i >= nx+NG-1 copying nx+NG-2 (likewise in y and z).
+static void set_inflow(const Dims &D, long p, double *Q, double *U, double *rhoi, double *Yi,
+                       const FlameThermo *th, const FlameInflow *in) {
+    const long np = D.np;
+    const int ns = D.ns;
+    for (int n = 0; n < ns; ++n) Yi[p + n * np] = 0.0, rhoi[p + n * np] = 0.0;
+    for (int n = 0; n < ns; ++n) Yi[p + n * np] = in->Y[n];
+    double yow = 0;  // ρmixture, thermo.jl:29-35
+    for (int n = 0; n < ns; ++n) yow += Yi[p + n * np] / th->mw[n];
+    const double rho = in->P / (th->Ru * in->T * yow);
+    double r[FLAME_MAX_NS];
+    for (int n = 0; n < ns; ++n) rhoi[p + n * np] = Yi[p + n * np] * rho, r[n] = rhoi[p + n * np];
+    const double ei = InternalEnergy(in->T, r, th, ns);
+    const double u = in->u, v = in->v, w = in->w;
+    const double q[7] = {rho, u, v, w, in->P, in->T, ei};
+    for (int n = 0; n < 7; ++n) Q[p + n * np] = q[n];
+    U[p] = rho;
+    U[p + np] = u * rho;
+    U[p + 2 * np] = v * rho;
+    U[p + 3 * np] = w * rho;
+    U[p + 4 * np] = ei + 0.5 * rho * (u * u + v * v + w * w);
+}
+
+static void copy_point(const Dims &D, long dst, long src, double *Q, double *U, double *rhoi) {
+    if (Q)
+        for (int n = 0; n < 7; ++n) Q[dst + n * D.np] = Q[src + n * D.np];
+    if (U)
+        for (int n = 0; n < 5; ++n) U[dst + n * D.np] = U[src + n * D.np];
+    if (rhoi)
+        for (int n = 0; n < D.ns; ++n) rhoi[dst + n * D.np] = rhoi[src + n * D.np];
+}
+
+// boundary.jl:1-52
+void oracle_fill_x(const FlameGrid *g, double *Q, double *U, double *rhoi, double *Yi,
+                   const FlameThermo *th, const FlameInflow *in, int rank, int nprocs) {
+    Dims D(g);
+    for (long k = 0; k < D.tz; ++k)
+        for (long j = 0; j < D.ty; ++j)
+            for (long i = 0; i < D.tx; ++i) {
+                const long p = D.P(i, j, k);
+                if (rank == 0 && i <= D.ng) set_inflow(D, p, Q, U, rhoi, Yi, th, in);
+                if (rank == nprocs - 1 && i >= D.nx + D.ng - 1)
+                    copy_point(D, p, D.P(D.nx + D.ng - 2, j, k), Q, U, rhoi);
+            }
+}
+
+// boundary.jl:54-80 (Q, U) and 139-158 (ρi alone: Q = U = null)
+void oracle_fill_y(const FlameGrid *g, double *Q, double *U, double *rhoi) {
+    Dims D(g);
+    for (long k = 0; k < D.tz; ++k)
+        for (long j = 0; j < D.ty; ++j)
+            for (long i = 0; i < D.tx; ++i) {
+                if (j <= D.ng)
+                    copy_point(D, D.P(i, j, k), D.P(i, D.ng + 1, k), Q, U, rhoi);
+                else if (j >= D.ny + D.ng - 1)
+                    copy_point(D, D.P(i, j, k), D.P(i, D.ny + D.ng - 2, k), Q, U, rhoi);
+            }
+}
+
+// boundary.jl:82-137
+void oracle_fill_z(const FlameGrid *g, double *Q, double *U, double *rhoi, double *Yi,
+                   const FlameThermo *th, const FlameInflow *in) {
+    Dims D(g);
+    for (long k = 0; k < D.tz; ++k)
+        for (long j = 0; j < D.ty; ++j)
+            for (long i = 0; i < D.tx; ++i) {
+                const long p = D.P(i, j, k);
+                if (k <= D.ng)
+                    set_inflow(D, p, Q, U, rhoi, Yi, th, in);
+                else if (k >= D.nz + D.ng - 1)
+                    copy_point(D, p, D.P(i, j, D.nz + D.ng - 2), Q, U, nullptr);
+            }
+}
+
+// boundary.jl:160-176
+void oracle_fill_z_s(const FlameGrid *g, double *rhoi) {
+    Dims D(g);
+    for (long k = D.nz + D.ng - 1; k < D.tz; ++k)
+        for (long j = 0; j < D.ty; ++j)
+            for (long i = 0; i < D.tx; ++i)
+                copy_point(D, D.P(i, j, k), D.P(i, j, D.nz + D.ng - 2), nullptr, nullptr, rhoi);
+}
+
+// The CFL rate max over interior cells of Σ_d J (|m_d·u| + c |m_d|) (this project's dt rule;
+// the reference runs a fixed dt, run.jl:30).
+double oracle_cfl_max(const FlameGrid *g, const double *Q, const FlameMetrics *m) {
+    Dims D(g);
+    const long np = D.np;
+    const double *rows[3][3] = {{m->dxidx, m->dxidy, m->dxidz},
+                                {m->detadx, m->detady, m->detadz},
+                                {m->dzetadx, m->dzetady, m->dzetadz}};
+    double best = 0;
+    for (long k = D.ng; k < D.nz + D.ng; ++k)
+        for (long j = D.ng; j < D.ny + D.ng; ++j)
+            for (long i = D.ng; i < D.nx + D.ng; ++i) {
+                const long p = D.P(i, j, k);
+                const double rho = Q[p], u = Q[p + np], v = Q[p + 2 * np], w = Q[p + 3 * np],
+                             pr = Q[p + 4 * np], e = Q[p + 6 * np];
+                const double gam = pr / e + 1;
+                const double cs = std::sqrt(gam * pr / rho);
+                const double J = m->J[p];
+                double tot = 0;
+                for (int d = 0; d < 3; ++d) {
+                    const double mx = rows[d][0][p], my = rows[d][1][p], mz = rows[d][2][p];
+                    tot += J * (std::fabs(mx * u + my * v + mz * w) +
+                                cs * std::sqrt(mx * mx + my * my + mz * mz));
+                }
+                best = jmax(best, tot);
+            }
+    return best;
+}
+
 // One SSP-RK3 stage exactly as solver.jl:298-326 orders it (IBM off, periodic fill in place of
 // the case-specific fillGhost/fillSpec).  All arrays are host arrays the caller owns.
 struct OracleState {

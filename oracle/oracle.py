@@ -56,12 +56,17 @@ SIGS = {
     "oracle_prim2c": [G, P, P],
     "oracle_mixture": [G, P, P, P, P, P, P, TH, TR, P],
     "oracle_fill_periodic": [G, P, I],
+    "oracle_fill_x": [G, P, P, P, P, TH, C.POINTER(abi.FlameInflow), I, I],
+    "oracle_fill_y": [G, P, P, P],
+    "oracle_fill_z": [G, P, P, P, P, TH, C.POINTER(abi.FlameInflow)],
+    "oracle_fill_z_s": [G, P],
     "oracle_rk_stage_seq": [G, I, D, P, P, P, P, P, M, TH, TR],
     "oracle_h_specs": [P, D, TH, I],
     "oracle_up7": [P],
 }
 RESTYPES = {"oracle_GetT": (D, [D, P, TH, I]), "oracle_InternalEnergy": (D, [D, P, TH, I]),
-            "oracle_CP": (D, [D, P, TH, I]), "oracle_num_threads": (C.c_int, [])}
+            "oracle_CP": (D, [D, P, TH, I]), "oracle_num_threads": (C.c_int, []),
+            "oracle_cfl_max": (D, [G, P, M])}
 
 _cache: dict[str, C.CDLL] = {}
 

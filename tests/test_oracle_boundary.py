@@ -1,0 +1,112 @@
+"""The oracle's restatement of the reference's ghost fills (boundary.jl:1-191) and of the CFL
+rate reduction, checked against their definitions on the host (no GPU)."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+
+def _state(f3d, ns=5, seed=21):
+    case = f3d.random_curvilinear(n=10, ns=ns, seed=seed)
+    Q = np.ascontiguousarray(case.Q.copy())
+    rhoi = np.ascontiguousarray(case.rhoi.copy())
+    U = np.ascontiguousarray(case.U())
+    Yi = np.ascontiguousarray(np.random.default_rng(seed).uniform(0, 1, rhoi.shape))
+    return case, Q, U, rhoi, Yi
+
+
+def test_fill_x_inflow_and_outlet(f3d, oracle):
+    case, Q, U, rhoi, Yi = _state(f3d)
+    Q0, U0, r0 = Q.copy(), U.copy(), rhoi.copy()
+    th = case.thermo.to_c()
+    inflow = f3d.cases.reference_inflow(case.ns)
+    lib = oracle.load()
+    P = oracle.ptr
+    lib.oracle_fill_x(C.byref(case.grid()), P(Q), P(U), P(rhoi), P(Yi), C.byref(th),
+                      C.byref(inflow), 0, 1)
+    NG, nx = f3d.FLAME_NG, case.nx
+    W = case.thermo.mw
+    Y = np.zeros(case.ns)
+    Y[1], Y[4] = 0.233, 0.767
+    rho = 79.8 / (case.thermo.Ru * 270.65 * np.sum(Y / W))
+    e = case.thermo.internal_energy(np.array([270.65]), (Y * rho)[:, None])[0]
+    inl = Q[:, :, :, :NG + 1]                       # i <= NG+1 (1-based)
+    assert np.allclose(inl[0], rho, rtol=1e-15) and np.all(inl[1] == 1000.0)
+    assert np.all(inl[2] == 0) and np.all(inl[3] == 0) and np.all(inl[4] == 79.8)
+    assert np.all(inl[5] == 270.65) and np.allclose(inl[6], e, rtol=1e-14)
+    assert np.allclose(U[4, :, :, :NG + 1], e + 0.5 * rho * 1e6, rtol=1e-14)
+    assert np.allclose(rhoi[:, :, :, 0], (Y * rho)[:, None, None], rtol=1e-15)
+    assert np.all(Yi[:, :, :, 0] == Y[:, None, None])
+    src = nx + NG - 2                               # Nxp+NG-1 (1-based)
+    for a, a0 in ((Q, Q0), (U, U0), (rhoi, r0)):
+        assert np.array_equal(a[..., nx + NG - 1:], np.repeat(a0[..., src:src + 1], NG + 1, -1))
+        assert np.array_equal(a[..., NG + 1:src + 1], a0[..., NG + 1:src + 1])  # untouched
+
+
+def test_fill_x_ranks(f3d, oracle):
+    """Middle ranks of an x-slab decomposition fill nothing; the last one only the outlet."""
+    case, Q, U, rhoi, Yi = _state(f3d)
+    Q0 = Q.copy()
+    th, inflow = case.thermo.to_c(), f3d.cases.reference_inflow(case.ns)
+    lib, P = oracle.load(), oracle.ptr
+    lib.oracle_fill_x(C.byref(case.grid()), P(Q), P(U), P(rhoi), P(Yi), C.byref(th),
+                      C.byref(inflow), 1, 3)
+    assert np.array_equal(Q, Q0)
+    lib.oracle_fill_x(C.byref(case.grid()), P(Q), P(U), P(rhoi), P(Yi), C.byref(th),
+                      C.byref(inflow), 2, 3)
+    NG = f3d.FLAME_NG
+    assert np.array_equal(Q[..., :NG + 1], Q0[..., :NG + 1])  # no inflow off rank 0
+
+
+def test_fill_y_and_z_zero_gradient(f3d, oracle):
+    case, Q, U, rhoi, Yi = _state(f3d, seed=22)
+    Q0, U0, r0 = Q.copy(), U.copy(), rhoi.copy()
+    lib, P, g = oracle.load(), oracle.ptr, C.byref(case.grid())
+    NG, ny, nz = f3d.FLAME_NG, case.ny, case.nz
+    lib.oracle_fill_y(g, P(Q), P(U), None)
+    for a, a0 in ((Q, Q0), (U, U0)):
+        assert np.array_equal(a[:, :, :NG + 1, :], np.repeat(a0[:, :, NG + 1:NG + 2, :], NG + 1, 2))
+        s = ny + NG - 2
+        assert np.array_equal(a[:, :, ny + NG - 1:, :], np.repeat(a0[:, :, s:s + 1, :], NG + 1, 2))
+    assert np.array_equal(rhoi, r0)  # fill_y leaves ρi to fill_y_s
+    lib.oracle_fill_y(g, None, None, P(rhoi))
+    assert np.array_equal(rhoi[:, :, :NG + 1, :], np.repeat(r0[:, :, NG + 1:NG + 2, :], NG + 1, 2))
+    r1 = rhoi.copy()
+    lib.oracle_fill_z_s(g, P(rhoi))
+    s = nz + NG - 2
+    assert np.array_equal(rhoi[:, nz + NG - 1:], np.repeat(r1[:, s:s + 1], NG + 1, 1))
+    assert np.array_equal(rhoi[:, :nz + NG - 1], r1[:, :nz + NG - 1])
+
+
+def test_fill_z_inflow(f3d, oracle):
+    case, Q, U, rhoi, Yi = _state(f3d, seed=23)
+    Q0 = Q.copy()
+    th, inflow = case.thermo.to_c(), f3d.cases.reference_inflow(case.ns)
+    lib, P = oracle.load(), oracle.ptr
+    lib.oracle_fill_z(C.byref(case.grid()), P(Q), P(U), P(rhoi), P(Yi), C.byref(th),
+                      C.byref(inflow))
+    NG, nz = f3d.FLAME_NG, case.nz
+    assert np.all(Q[1, :NG + 1] == 1000.0) and np.all(Q[4, :NG + 1] == 79.8)
+    s = nz + NG - 2
+    assert np.array_equal(Q[:, nz + NG - 1:], np.repeat(Q0[:, s:s + 1], NG + 1, 1))
+
+
+def test_reference_inflow_needs_five_species(f3d):
+    with pytest.raises(ValueError):
+        f3d.cases.reference_inflow(3)
+
+
+@pytest.mark.parametrize("maker", ["jet", "rand", "tgv"])
+def test_cfl_max_matches_host_rule(f3d, oracle, maker):
+    case = {"jet": lambda: f3d.curvilinear_jet(nx=24, ny=16, nz=12),
+            "rand": lambda: f3d.random_curvilinear(n=12, ns=3, seed=24),
+            "tgv": lambda: f3d.taylor_green(n=16, Ma=0.4)}[maker]()
+    m = {k: np.ascontiguousarray(v) for k, v in case.metrics.items()}
+    rate = oracle.load().oracle_cfl_max(C.byref(case.grid()), oracle.ptr(np.ascontiguousarray(case.Q)),
+                                        C.byref(oracle.metrics_struct(m)))
+    cfl = case.info.get("cfl", 0.5)
+    assert cfl / rate == case.dt  # the same rule, the same operation order, bit for bit
+    assert math.isfinite(rate) and rate > 0
