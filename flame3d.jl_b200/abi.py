@@ -44,7 +44,7 @@ class FlameThermo(C.Structure):
 class FlameTransport(C.Structure):
     _fields_ = [("law", C.c_int32), ("pad", C.c_int32), ("mu_ref", C.c_double),
                 ("T_ref", C.c_double), ("exponent", C.c_double), ("Pr", C.c_double),
-                ("lambda_ref", C.c_double), ("D_ref", C.c_double)]
+                ("lambda_ref", C.c_double), ("D_ref", C.c_double), ("poly", C.c_void_p)]
 
 
 METRIC_NAMES = ("dxidx", "dxidy", "dxidz", "detadx", "detady", "detadz",

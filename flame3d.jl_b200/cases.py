@@ -121,7 +121,9 @@ def synthetic_species(ns: int = 9, seed: int = 3) -> Thermo:
 @dataclass
 class Transport:
     """law 0: constants; law 1: mu = mu_ref (T/T_ref)^exponent, lambda = cp mu / Pr,
-    D = lambda / (rho cp) (unity Lewis)."""
+    D = lambda / (rho cp) (unity Lewis); law 2: the reference's mixture-averaged properties
+    (thermo.jl:289-369) from the log(T) fits in `poly` (visc (5, ns) | conduct (5, ns) |
+    binarydiff (5, ns, ns), each column-major, flattened back to back)."""
     law: int = 1
     mu_ref: float = 1.8e-5
     T_ref: float = 300.0
@@ -129,12 +131,51 @@ class Transport:
     Pr: float = 0.71
     lambda_ref: float = 0.0
     D_ref: float = 0.0
+    poly: np.ndarray | None = None
 
-    def to_c(self) -> FlameTransport:
+    def to_c(self, poly_ptr: int | None = None) -> FlameTransport:
+        """The C struct; for law 2 `poly_ptr` is the address of `poly` where the callee reads
+        it (a device copy for the GPU, the host array for the oracle)."""
         t = FlameTransport()
         t.law, t.mu_ref, t.T_ref, t.exponent = self.law, self.mu_ref, self.T_ref, self.exponent
         t.Pr, t.lambda_ref, t.D_ref = self.Pr, self.lambda_ref, self.D_ref
+        if self.law == 2:
+            if poly_ptr is None:
+                poly_ptr = self.poly.ctypes.data  # host: the array itself
+            t.poly = poly_ptr
         return t
+
+
+def _fit_log_poly(T: np.ndarray, f: np.ndarray) -> np.ndarray:
+    """Least-squares quartic in ln T, coefficients in ascending order (dot5, thermo.jl:284)."""
+    return np.polynomial.polynomial.polyfit(np.log(T), f, 4)
+
+
+def mixture_averaged_transport(thermo: Thermo, seed: int = 9) -> Transport:
+    """Seeded log(T) fits in the form initThermo takes from Cantera (thermo.jl:405-436), for law
+    2.  Per species μ_k = μ0_k (T/300)^0.7, μ0_k ~ U[1, 3]·1e-5 Pa s, fitted as sqrt(μ/√T);
+    λ_k = λ0_k (T/300)^0.8, λ0_k ~ U[0.02, 0.2] W/(m K), fitted as λ/√T; binary diffusion
+    P·D_jk = d_jk (T/300)^1.75, d_jk = d_kj ~ U[1, 4] Pa m²/s, fitted as P·D/T^1.5; all over
+    200-3000 K."""
+    ns = thermo.ns
+    rng = np.random.default_rng(seed)
+    T = np.linspace(200.0, 3000.0, 64)
+    visc = np.zeros((ns, 5))
+    cond = np.zeros((ns, 5))
+    binc = np.zeros((ns, ns, 5))
+    mu0 = rng.uniform(1e-5, 3e-5, ns)
+    lam0 = rng.uniform(0.02, 0.2, ns)
+    d0 = rng.uniform(1.0, 4.0, (ns, ns))
+    d0 = 0.5 * (d0 + d0.T)
+    for k in range(ns):
+        mu = mu0[k] * (T / 300.0) ** 0.7
+        visc[k] = _fit_log_poly(T, np.sqrt(mu / np.sqrt(T)))
+        cond[k] = _fit_log_poly(T, lam0[k] * (T / 300.0) ** 0.8 / np.sqrt(T))
+        for j in range(ns):
+            binc[k, j] = _fit_log_poly(T, d0[j, k] * (T / 300.0) ** 1.75 / T ** 1.5)
+    # column-major (5, ns) and (5, ns, ns): coefficient fastest, then the first species index
+    poly = np.concatenate([visc.ravel(), cond.ravel(), binc.ravel()])
+    return Transport(law=2, poly=np.ascontiguousarray(poly))
 
 
 # ------------------------------------------------------------------------------------- grids

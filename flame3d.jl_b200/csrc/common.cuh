@@ -309,6 +309,64 @@ __device__ __forceinline__ T hybrid_face7(const T *p, const T *m, T phif) {
     return fp + fm;
 }
 
+// ---- mixtureProperties, thermo.jl:284-369 (transport law 2) in the reference's order.
+// dot5, thermo.jl:284-286
+__device__ __forceinline__ double dot5(double l1, double l2, double l3, double l4,
+                                       const double *p) {
+    return p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3] + l4 * p[4];
+}
+
+// X: mole fractions; poly: visc (5, ns) | conduct (5, ns) | binarydiff (5, ns, ns).  Writes the
+// mixture-averaged D_k to Dk[n * stride] and returns λ, μ.  W is an ns*ns work array.
+__device__ __forceinline__ void mixture_properties(double T, double P, const double *X,
+                                                   const FlameThermo &th, const double *poly,
+                                                   int ns, double *W, double *mui, double *Dk,
+                                                   long long stride, double &lam, double &mu) {
+    const double *visc = poly, *cond = poly + 5 * ns, *bin = poly + 10 * ns;
+    const double sqT = sqrt(T), sqsqT = sqrt(sqT), lgT = log(T);
+    const double lgT2 = lgT * lgT, lgT3 = lgT * lgT2, lgT4 = lgT2 * lgT2;
+    for (int n = 0; n < ns; ++n) mui[n] = sqT * dot5(lgT, lgT2, lgT3, lgT4, cond + 5 * n);
+    double sum1 = 0, sum2 = 0;
+    for (int k = 0; k < ns; ++k) sum1 += X[k] * mui[k], sum2 += X[k] / mui[k];
+    lam = 0.5 * (sum1 + 1 / sum2);
+    for (int n = 0; n < ns; ++n) {
+        const double s = sqsqT * dot5(lgT, lgT2, lgT3, lgT4, visc + 5 * n);
+        mui[n] = s * s;
+    }
+    for (int n = 0; n < ns; ++n) {  // Wilke, W[n*ns + l] is the reference's D[(n-1)*Nspecs+l]
+        const double tmp1 = 1 / th.mw[n], tmp2 = mui[n];
+        for (int l = 0; l <= n; ++l) {
+            const double wr = th.mw[l] * tmp1, vr = tmp2 / mui[l];
+            const double f1 = 1 + sqrt(vr * sqrt(wr));
+            const double t = f1 * f1 / sqrt(8 + 8 / wr);
+            W[n * ns + l] = t;
+            W[l * ns + n] = t / (vr * wr);
+        }
+        W[n * ns + n] = 1.0;
+    }
+    mu = 0;
+    for (int n = 0; n < ns; ++n) {
+        double t = 0.0;
+        for (int l = 0; l < ns; ++l) t += X[l] * W[n * ns + l];
+        mu += X[n] * mui[n] / t;
+    }
+    for (int n = 0; n < ns; ++n)
+        for (int m = n; m < ns; ++m) {
+            const double t = T * sqT * dot5(lgT, lgT2, lgT3, lgT4, bin + 5 * (m + ns * n));
+            W[m * ns + n] = t;
+            W[n * ns + m] = t;
+        }
+    for (int n = 0; n < ns; ++n) {
+        double s = 0.0;
+        for (int m = 0; m < ns; ++m) {
+            if (m == n) continue;
+            s += X[m] / W[n * ns + m];
+        }
+        s *= P;
+        Dk[n * stride] = (1 - X[n]) / (s + kEps);
+    }
+}
+
 }  // namespace flame
 
 // Error plumbing shared by every C entry point (defined in capi.cu).

@@ -664,6 +664,10 @@ extern "C" int flame_transport(const FlameGrid *g, flame_stream_t s, const void 
     if (int e = check_sizes(g, "flame_transport")) return e;
     if (!Q || !rhoi || !trans || !th || !tr)
         return flame_fail(FLAME_EINVAL, "flame_transport: NULL argument");
+    if (tr->law == 2)
+        return flame_fail(FLAME_EUNSUPPORTED,
+                          "flame_transport: law 2 (mixture-averaged, per-species D_k) runs on the "
+                          "per-kernel path (flame_mixture); the fused stage takes laws 0 and 1");
     if (tr->law != 0 && tr->law != 1)
         return flame_fail(FLAME_EINVAL, "flame_transport: transport law %d unknown", tr->law);
     const int np = (g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
@@ -687,6 +691,10 @@ extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int st
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: NULL argument");
     if (stage < 1 || stage > 3)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: stage=%d must be 1, 2 or 3", stage);
+    if (tr->law != 0 && tr->law != 1)
+        return flame_fail(tr->law == 2 ? FLAME_EUNSUPPORTED : FLAME_EINVAL,
+                          "flame_rk_stage: transport law %d; the fused stage takes laws 0 and 1 "
+                          "(law 2 runs on the per-kernel path)", tr->law);
     if ((g->periodic & 7) != 7)
         return flame_fail(FLAME_EUNSUPPORTED,
                           "flame_rk_stage: the fused stage needs a grid periodic in x, y and z; "

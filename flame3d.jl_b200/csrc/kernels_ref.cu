@@ -380,6 +380,16 @@ __global__ void k_mixture(Dims D, const double *__restrict__ Q, const double *__
         Yi[c + n * np] = Y[n];
     }
     double mv, lv, dv;
+    if (tr.law == 2) {  // Y2X (thermo.jl:38-52), then mixtureProperties
+        double yow = 0;
+        for (int n = 0; n < ns; ++n) yow += Y[n] / th.mw[n];
+        const double yowinv = 1 / yow;
+        double X[FLAME_MAX_NS], mui[FLAME_MAX_NS], W[FLAME_MAX_NS * FLAME_MAX_NS];
+        for (int n = 0; n < ns; ++n) X[n] = Y[n] / th.mw[n] * yowinv;
+        mixture_properties(T, Q[c + 4 * np], X, th, tr.poly, ns, W, mui, Dk + c, np, lv, mv);
+        mu[c] = mv, lambda[c] = lv;
+        return;
+    }
     if (tr.law == 0) {
         mv = tr.mu_ref, lv = tr.lambda_ref, dv = tr.D_ref;
     } else {
@@ -704,8 +714,10 @@ int flame_mixture(const FlameGrid *g, flame_stream_t s, const double *Q, const d
     if (int e = flame_check_grid(g, "flame_mixture")) return e;
     if (!Q || !rhoi || !Yi || !lambda || !mu || !Dk || !th || !tr)
         return flame_fail(FLAME_EINVAL, "flame_mixture: NULL argument");
-    if (tr->law != 0 && tr->law != 1)
+    if (tr->law < 0 || tr->law > 2)
         return flame_fail(FLAME_EINVAL, "flame_mixture: transport law %d unknown", tr->law);
+    if (tr->law == 2 && !tr->poly)
+        return flame_fail(FLAME_EINVAL, "flame_mixture: law 2 needs the polynomial fits (poly)");
     Dims D = make_dims(*g);
     k_mixture<<<(unsigned)((D.np + 255) / 256), 256, 0, s>>>(D, Q, rhoi, Yi, lambda, mu, Dk, *th,
                                                               *tr, tag);

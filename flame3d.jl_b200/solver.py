@@ -41,7 +41,12 @@ class DeviceCase:
         self.precision = precision
         self.grid = case.grid()
         self.thermo = case.thermo.to_c()
-        self.transport = case.transport.to_c()
+        self.poly = None  # law 2: the transport fits, on the device
+        if case.transport.law == 2:
+            self.poly = torch.as_tensor(case.transport.poly, dtype=torch.float64).to(self.device)
+            self.transport = case.transport.to_c(self.poly.data_ptr())
+        else:
+            self.transport = case.transport.to_c()
         self.dt = case.dt
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
@@ -72,15 +77,18 @@ class DeviceCase:
             self._call("flame_prim2c", _p(self.U), _p(up(case.Q)))
         else:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
-        self._transport()
         self.scratch = None
         self.seq = None
-        # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice, or
-        # None for the pencil sweeps (configuration 3)
-        self.set_tile(3 if tile is None or tile == "auto" else tile)
-        if tile == "auto":
-            from . import autotune
-            self.set_tile(autotune.default().choose(self))
+        if case.transport.law == 2:  # per-species D_k: the launch sequence only
+            self.tile = None
+        else:
+            self._transport()
+            # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice,
+            # or None for the pencil sweeps (configuration 3)
+            self.set_tile(3 if tile is None or tile == "auto" else tile)
+            if tile == "auto":
+                from . import autotune
+                self.set_tile(autotune.default().choose(self))
         if sequence_buffers:
             self._alloc_sequence()
 
@@ -99,7 +107,7 @@ class DeviceCase:
         them), optionally with another configuration."""
         c = DeviceCase.__new__(DeviceCase)
         for a in ("lib", "case", "device", "precision", "grid", "thermo", "transport", "dt",
-                  "metrics", "cmetrics", "cur"):
+                  "metrics", "cmetrics", "cur", "poly"):
             setattr(c, a, getattr(self, a))
         c.Q = [q.clone() for q in self.Q]
         c.rhoi = [r.clone() for r in self.rhoi]

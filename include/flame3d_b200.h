@@ -65,14 +65,22 @@ typedef struct FlameThermo {
     double coeffs_hi[7 * FLAME_MAX_NS];
 } FlameThermo;
 
-/* Transport law that stands in for Cantera's mixture-averaged fits (thermo.jl:289-403).
+/* Transport law (thermo.jl:289-403).
  *   law 0: mu = mu_ref, lambda = lambda_ref, D_k = D_ref (constants)
  *   law 1: mu = mu_ref * (T / T_ref)^exponent, lambda = cp * mu / Pr with cp the mass-specific
- *          mixture heat capacity, D_k = lambda / (rho * cp) for every species (unity Lewis). */
+ *          mixture heat capacity, D_k = lambda / (rho * cp) for every species (unity Lewis).
+ *   law 2: the reference's mixture-averaged properties, mixtureProperties thermo.jl:289-369:
+ *          Mathur lambda, Wilke mu and mixture-averaged D_k from the log(T) polynomial fits
+ *          that initThermo takes from Cantera (thermo.jl:405-436), here supplied by the
+ *          caller in `poly`: visc_poly (5, ns), conduct_poly (5, ns), binarydiff_poly
+ *          (5, ns, ns), each column-major as in thermoProperty, back to back (10 ns + 5 ns^2
+ *          doubles, device memory for the GPU entry points).  Laws 0 and 1 run everywhere;
+ *          law 2 runs on the per-kernel path (flame_mixture), whose D_k are per species. */
 typedef struct FlameTransport {
     int32_t law;
     int32_t pad;
     double mu_ref, T_ref, exponent, Pr, lambda_ref, D_ref;
+    const double *poly; /* law 2 only */
 } FlameTransport;
 
 /* Curvilinear metrics (J^-1-scaled cofactors, parse_mesh.jl:210-221) and J, all ghosted. */

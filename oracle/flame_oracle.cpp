@@ -617,6 +617,62 @@ void oracle_prim2c(const FlameGrid *g, double *U, const double *Q) {
 }
 
 // thermo.jl:371-403 mixture(), with the FlameTransport law in place of Cantera's fits.
+// mixtureProperties, thermo.jl:284-369 (transport law 2): Mathur λ, Wilke μ, mixture-averaged
+// D_k from the log(T) fits; poly = visc (5, ns) | conduct (5, ns) | binarydiff (5, ns, ns).
+static double dot5(double l1, double l2, double l3, double l4, const double *p) {
+    return p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3] + l4 * p[4];
+}
+
+void oracle_mixture_properties(double T, double P, const double *X, const FlameThermo *th,
+                               const double *poly, int ns, double *Dk, double *lam_out,
+                               double *mu_out) {
+    const double *visc = poly, *cond = poly + 5 * ns, *bin = poly + 10 * ns;
+    double mui[FLAME_MAX_NS], W[FLAME_MAX_NS * FLAME_MAX_NS];
+    const double sqT = std::sqrt(T), sqsqT = std::sqrt(sqT), lgT = std::log(T);
+    const double lgT2 = lgT * lgT, lgT3 = lgT * lgT2, lgT4 = lgT2 * lgT2;
+    for (int n = 0; n < ns; ++n) mui[n] = sqT * dot5(lgT, lgT2, lgT3, lgT4, cond + 5 * n);
+    double sum1 = 0, sum2 = 0;
+    for (int k = 0; k < ns; ++k) sum1 += X[k] * mui[k], sum2 += X[k] / mui[k];
+    *lam_out = 0.5 * (sum1 + 1 / sum2);
+    for (int n = 0; n < ns; ++n) {
+        const double sq = sqsqT * dot5(lgT, lgT2, lgT3, lgT4, visc + 5 * n);
+        mui[n] = sq * sq;
+    }
+    for (int n = 0; n < ns; ++n) {  // Wilke, Poling et al. (2001) eq. 9-5.14
+        const double tmp1 = 1 / th->mw[n], tmp2 = mui[n];
+        for (int l = 0; l <= n; ++l) {
+            const double wr = th->mw[l] * tmp1, vr = tmp2 / mui[l];
+            const double f1 = 1 + std::sqrt(vr * std::sqrt(wr));
+            const double t = f1 * f1 / std::sqrt(8 + 8 / wr);
+            W[n * ns + l] = t;
+            W[l * ns + n] = t / (vr * wr);
+        }
+        W[n * ns + n] = 1.0;
+    }
+    double mu = 0;
+    for (int n = 0; n < ns; ++n) {
+        double t = 0.0;
+        for (int l = 0; l < ns; ++l) t += X[l] * W[n * ns + l];
+        mu += X[n] * mui[n] / t;
+    }
+    *mu_out = mu;
+    for (int n = 0; n < ns; ++n)
+        for (int m = n; m < ns; ++m) {
+            const double t = T * sqT * dot5(lgT, lgT2, lgT3, lgT4, bin + 5 * (m + ns * n));
+            W[m * ns + n] = t;
+            W[n * ns + m] = t;
+        }
+    for (int n = 0; n < ns; ++n) {
+        double sm = 0.0;
+        for (int m = 0; m < ns; ++m) {
+            if (m == n) continue;
+            sm += X[m] / W[n * ns + m];
+        }
+        sm *= P;
+        Dk[n] = (1 - X[n]) / (sm + kEps);
+    }
+}
+
 void oracle_mixture(const FlameGrid *g, const double *Q, const double *rhoi, double *Yi,
                     double *lambda, double *mu, double *Dk, const FlameThermo *th,
                     const FlameTransport *tr, const int64_t *tag) {
@@ -635,6 +691,18 @@ void oracle_mixture(const FlameGrid *g, const double *Q, const double *rhoi, dou
             Yi[c + n * np] = Y[n];
         }
         double m, l, dd;
+        if (tr->law == 2) {  // Y2X, thermo.jl:38-52
+            double yow = 0;
+            for (int n = 0; n < ns; ++n) yow += Y[n] / th->mw[n];
+            const double yowinv = 1 / yow;
+            double X[FLAME_MAX_NS], Dl[FLAME_MAX_NS];
+            for (int n = 0; n < ns; ++n) X[n] = Y[n] / th->mw[n] * yowinv;
+            oracle_mixture_properties(T, Q[c + 4 * np], X, th, tr->poly, ns, Dl, &l, &m);
+            mu[c] = m;
+            lambda[c] = l;
+            for (int n = 0; n < ns; ++n) Dk[c + n * np] = Dl[n];
+            continue;
+        }
         if (tr->law == 0) {
             m = tr->mu_ref, l = tr->lambda_ref, dd = tr->D_ref;
         } else {

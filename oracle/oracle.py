@@ -60,6 +60,7 @@ SIGS = {
     "oracle_fill_y": [G, P, P, P],
     "oracle_fill_z": [G, P, P, P, P, TH, C.POINTER(abi.FlameInflow)],
     "oracle_fill_z_s": [G, P],
+    "oracle_mixture_properties": [D, D, P, TH, P, I, P, P, P],
     "oracle_rk_stage_seq": [G, I, D, P, P, P, P, P, M, TH, TR],
     "oracle_h_specs": [P, D, TH, I],
     "oracle_up7": [P],
