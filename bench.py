@@ -410,6 +410,26 @@ def run_serve(args, f3d) -> int:
     return 0
 
 
+# ------------------------------------------------------------------------------ replicas
+def max_over_ranks(ms: float, device=None) -> float:
+    """The slowest rank's time: N replicas are done when the last one is (all_reduce MAX; on
+    one process the time itself).  `device` is where the collective's tensor lives (the rank's
+    GPU under NCCL, the CPU under gloo)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(cells: int, stages: int, ms_max: float, world: int) -> float:
+    """Whole-job Mcell-stage/s of `world` replicas that each ran `stages` stages of `cells`
+    cells, finished when the slowest did (weak scaling: per-rank work fixed)."""
+    return world * cells * stages / (ms_max / 1e3) / 1e6
+
+
 # ------------------------------------------------------------------------------ GPU side
 def main() -> int:
     ap = argparse.ArgumentParser()
@@ -479,14 +499,10 @@ def main() -> int:
     e1.record(stream)
     barrier()
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
     stages = 3 * args.steps
     cells = case.cells
-    value = world * cells * stages / (ms / 1e3) / 1e6
+    value = replica_rate(cells, stages, ms, world)
     stage_ms = ms / stages  # device time of one stage (all of its launches)
 
     # ---- end to end through the host-buffer API (pinned host memory, copies timed)
@@ -504,12 +520,8 @@ def main() -> int:
         dc.advance_from_host(Qh, rh, 1, Qo, ro)
     e1.record(stream)
     barrier()
-    ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * cells * 3 * e2e_steps / (ms_e2e / 1e3) / 1e6
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev)
+    e2e_value = replica_rate(cells, 3 * e2e_steps, ms_e2e, world)
     h2d = (Qh.numel() * Qh.element_size() + rh.numel() * rh.element_size())
     d2h = (Qo.numel() * Qo.element_size() + ro.numel() * ro.element_size())
 
