@@ -140,6 +140,78 @@ __device__ double get_T(const FlameThermo &th, int ns, double ein, const double 
     return t1;
 }
 
+// GetT for the fused stages: the same iteration as get_T (start, clamps, tolerance, break
+// before the update), with e(T) and cv(T) of the mixture evaluated from its own polynomial.
+// e/R and cv/R are linear in the species weights w_n = ρ_n / W_n, so the per-species NASA-7
+// coefficients are summed once per cell into the mixture's coefficients for the low and the
+// high range; an iteration then costs one polynomial instead of ns.  Where T lies between
+// separators of different species the per-species sums are used.  The result differs from
+// get_T by round-off only.
+template <int NS>
+struct MixPoly {
+    double lo[5], hi[5], off, smin, smax;  // e/R = Σ_a c_a T_a (+ off in the high range)
+    double wsum;                           // Σ_n w_n, so that Σ_n w_n cp_n = cv + Ru wsum
+    const FlameThermo *th;
+    const double *rhoi;
+    __device__ __forceinline__ MixPoly(const FlameThermo &t, const double *r) : th(&t), rhoi(r) {
+#pragma unroll
+        for (int a = 0; a < 5; ++a) lo[a] = 0.0, hi[a] = 0.0;
+        off = 0.0, wsum = 0.0;
+        smin = smax = t.coeffs_sep[0];
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            const double w = r[n] / t.mw[n];
+            wsum += w;
+            const double *L = t.coeffs_lo + 7 * n, *H = t.coeffs_hi + 7 * n;
+            lo[0] += w * (L[0] - 1), hi[0] += w * (H[0] - 1);
+#pragma unroll
+            for (int a = 1; a < 5; ++a) lo[a] += w * L[a], hi[a] += w * H[a];
+            off += w * (H[5] - L[5]);
+            smin = fmin(smin, t.coeffs_sep[n]), smax = fmax(smax, t.coeffs_sep[n]);
+        }
+    }
+    __device__ __forceinline__ double e(double T) const {  // InternalEnergy, J/m^3
+        if (T >= smin && T < smax) return internal_energy<NS>(*th, NS, T, rhoi);
+        const double T2 = 0.5 * T * T, T3 = 2.0 / 3.0 * T2 * T, T4 = T2 * T2, T5 = 0.8 * T4 * T;
+        const double *c = T < smin ? lo : hi;
+        const double r = c[0] * T + c[1] * T2 + c[2] * T3 + c[3] * T4 + c[4] * T5;
+        return (T < smin ? r : r + off) * th->Ru;
+    }
+    __device__ __forceinline__ double cv(double T) const {  // CV, J/(m^3 K)
+        if (T >= smin && T < smax) return heat_cv<NS>(*th, NS, T, rhoi);
+        const double *c = T < smin ? lo : hi;
+        const double T2 = T * T, T3 = T2 * T, T4 = T2 * T2;
+        return (c[0] + c[1] * T + c[2] * T2 + c[3] * T3 + c[4] * T4) * th->Ru;
+    }
+};
+
+template <int NS>
+__device__ double get_T_mix(const MixPoly<NS> &M, const FlameThermo &th, double ein,
+                            const double *rhoi) {
+    const double tol = 1e-3;
+    const double tmin = th.min_temp, tmax = th.max_temp;
+    const double emin = M.e(tmin), emax = M.e(tmax);
+    if (ein < emin) return tmin - (emin - ein) / M.cv(tmin);
+    if (ein > emax) return tmax - (emax - ein) / M.cv(tmax);
+    double As = 0;
+    for (int n = 0; n < NS; ++n) As += (th.coeffs_lo[7 * n] - 1) * th.Ru / th.mw[n] * rhoi[n];
+    double t1 = ein / As;
+    if (t1 < tmin || t1 > tmax) t1 = tmin + (tmax - tmin) / (emax - emin) * (ein - emin);
+    for (int it = 0; it < 30; ++it) {
+        double dt = (ein - M.e(t1)) / M.cv(t1);
+        if (dt > 100.0)
+            dt = 100.0;
+        else if (dt < -100.0)
+            dt = -100.0;
+        else if (fabs(dt) < tol)
+            break;
+        else if (t1 + dt == t1)
+            break;
+        t1 += dt;
+    }
+    return t1;
+}
+
 // Pmixture, thermo.jl:20-26
 template <int NS>
 __device__ __forceinline__ double p_mixture(const FlameThermo &th, int ns, double T,

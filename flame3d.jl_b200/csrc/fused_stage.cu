@@ -489,7 +489,9 @@ struct Tile {
             for (int n = 0; n < NS; ++n) r[n] *= sc;
             const double u = Uc[1] * rinv, v = Uc[2] * rinv, w = Uc[3] * rinv;
             const double ei = jmax(Uc[4] - 0.5 * rho * (u * u + v * v + w * w), kEps);
-            const double Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
+            const double Tn = jmax(NS < 4 ? get_T<NS>(A.th, NS, ei, r)
+                                           : get_T_mix<NS>(MixPoly<NS>(A.th, r), A.th, ei, r),
+                                   kEps);
             const double p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
             double mu, lam, D;
             transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);

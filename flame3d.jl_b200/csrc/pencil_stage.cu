@@ -235,6 +235,9 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 }
 
 // ---- phase B: the face between pencil positions l-1 and l; G = F_inviscid − F_viscous.
+// The species part runs one species at a time in two passes (the sums of the diffusion
+// velocities first, then each species' reconstruction, corrected diffusion flux and enthalpy
+// flux), recomputing the few gradient terms instead of holding per-species arrays in registers.
 template <int DIR, int NS, typename QT, typename CT>
 __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G) {
     using SL = Slots<NS>;
@@ -243,16 +246,15 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
 #define SV(slot, ll) S[(slot) * 32 + (ll)]
     const int lm = l - 1;
     const CT phif = CT(jmax(double(SV(SL::PHI, lm)), double(SV(SL::PHI, l))));
-#pragma unroll
-    for (int n = 0; n < 5 + NS; ++n) {
-        const int vp = n < 5 ? n : 5 + n;
-        const int vm = n < 5 ? 5 + n : 5 + NS + n;
+    auto recon = [&](int vp, int vm) {
         CT pv[7], mv[7];
 #pragma unroll
         for (int i = 0; i < 6; ++i) pv[i] = SV(vp, l - 3 + i), mv[i] = SV(vm, l - 3 + i);
         pv[6] = mv[6] = CT(0);
-        G[n] = hybrid_face_fast<CT>(pv, mv, phif);
-    }
+        return hybrid_face_fast<CT>(pv, mv, phif);
+    };
+#pragma unroll
+    for (int n = 0; n < 5; ++n) G[n] = recon(n, 5 + n);
     CT met[9];
 #pragma unroll
     for (int m = 0; m < 9; ++m) met[m] = (SV(SL::MET + m, lm) + SV(SL::MET + m, l)) * h;
@@ -263,24 +265,26 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
     const CT rho = (SV(SL::RHO, lm) + SV(SL::RHO, l)) * h;
     const CT Tf = (SV(SL::Q4 + 3, lm) + SV(SL::Q4 + 3, l)) * h;
     const CT *md = met + 3 * DIR;
-    // species diffusion (viscous.jl:430-507) first: it yields Fh for the energy flux
-    CT Vk1[NS], Vk2[NS], Vk3[NS], Yf[NS];
-    CT sum1 = 0, sum2 = 0, sum3 = 0;
-#pragma unroll
-    for (int n = 0; n < NS; ++n) {
+    // species diffusion (viscous.jl:430-507): the diffusion velocity of species n at the face
+    const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
+    auto diffusion = [&](int n, CT &Vx, CT &Vy, CT &Vz) {
         const CT y0 = SV(SL::Y + n, l), ym = SV(SL::Y + n, lm);
         const CT yp = SV(SL::Y + n, l + 1), ymm = SV(SL::Y + n, l - 2);
         CT dY[3];
         dY[DIR] = CT(1.25) * (y0 - ym) - c12 * (yp - ymm);
         dY[D1] = CT(0.25) * (SV(SL::DY1 + n, l) + SV(SL::DY1 + n, lm));
         dY[D2] = CT(0.25) * (SV(SL::DY2 + n, l) + SV(SL::DY2 + n, lm));
-        const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
-        const CT Vx = (dY[0] * met[0] + dY[1] * met[3] + dY[2] * met[6]) * Jac * rhoDi;
-        const CT Vy = (dY[0] * met[1] + dY[1] * met[4] + dY[2] * met[7]) * Jac * rhoDi;
-        const CT Vz = (dY[0] * met[2] + dY[1] * met[5] + dY[2] * met[8]) * Jac * rhoDi;
-        Vk1[n] = Vx, Vk2[n] = Vy, Vk3[n] = Vz;
+        Vx = (dY[0] * met[0] + dY[1] * met[3] + dY[2] * met[6]) * Jac * rhoDi;
+        Vy = (dY[0] * met[1] + dY[1] * met[4] + dY[2] * met[7]) * Jac * rhoDi;
+        Vz = (dY[0] * met[2] + dY[1] * met[5] + dY[2] * met[8]) * Jac * rhoDi;
+        return h * (ym + y0);
+    };
+    CT sum1 = 0, sum2 = 0, sum3 = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        CT Vx, Vy, Vz;
+        diffusion(n, Vx, Vy, Vz);
         sum1 += Vx, sum2 += Vy, sum3 += Vz;
-        Yf[n] = h * (ym + y0);
     }
     CT fh1 = 0, fh2 = 0, fh3 = 0;
     {
@@ -288,10 +292,11 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
         const double T2 = 0.5 * Td * Td, T3 = 2.0 / 3.0 * T2 * Td, T4 = T2 * T2, T5 = 0.8 * T4 * Td;
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
+            CT Vx, Vy, Vz;
+            const CT Yf = diffusion(n, Vx, Vy, Vz);
             const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
-            const CT V1 = Vk1[n] - sum1 * Yf[n], V2 = Vk2[n] - sum2 * Yf[n],
-                     V3 = Vk3[n] - sum3 * Yf[n];
-            G[5 + n] -= V1 * md[0] + V2 * md[1] + V3 * md[2];
+            const CT V1 = Vx - sum1 * Yf, V2 = Vy - sum2 * Yf, V3 = Vz - sum3 * Yf;
+            G[5 + n] = recon(10 + n, 10 + NS + n) - (V1 * md[0] + V2 * md[1] + V3 * md[2]);
             fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
         }
     }
@@ -363,10 +368,25 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     for (int n = 0; n < NS; ++n) r[n] *= sc;
     const double u = Uc[1] * rinv, v = Uc[2] * rinv, w = Uc[3] * rinv;
     const double ei = jmax(Uc[4] - 0.5 * rho * (u * u + v * v + w * w), kEps);
-    const double Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
-    const double p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
-    double mu, lam, D;
-    transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
+    double mu, lam, D, Tn, p;
+    if constexpr (NS < 4) {  // few species: the per-species sums are as cheap
+        Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
+        p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
+        transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
+    } else {  // the mixture's own polynomials (MixPoly): one evaluation per Newton iteration
+        const MixPoly<NS> M(A.th, r);
+        Tn = jmax(get_T_mix<NS>(M, A.th, ei, r), kEps);
+        p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
+        if (A.tr.law == 0) {
+            mu = A.tr.mu_ref, lam = A.tr.lambda_ref, D = A.tr.D_ref;
+        } else {  // transport_point with cp_mix = Σ_n w_n cp_n / ρ from the same polynomials
+            const double rh = jmax(rho, kEps);
+            const double cpm = (M.cv(Tn) + A.th.Ru * M.wsum) / rh;
+            mu = A.tr.mu_ref * pow(Tn / A.tr.T_ref, A.tr.exponent);
+            lam = cpm * mu / A.tr.Pr;
+            D = lam / (rh * cpm);
+        }
+    }
     const double qv[7] = {rho, u, v, w, p, Tn, ei};
     const double tv[3] = {mu, lam, D};
     // the cell and its periodic ghost images (new: the reference fills ghosts with case-specific

@@ -92,6 +92,13 @@ class DeviceCase:
         if sequence_buffers:
             self._alloc_sequence()
 
+    def restore_conserved(self, q64: torch.Tensor) -> None:
+        """After the primitive state was replaced (a restart): U from the FP64 primitives
+        (prim2c, utils.jl:71-92) and the transport of the state for the fused stage."""
+        self._call("flame_prim2c", _p(self.U), _p(q64.contiguous()))
+        if self.transport.law != 2:
+            self._transport()
+
     def set_tile(self, tile: int) -> None:
         """Switches the fused stage's configuration (the pencil ones need scratch)."""
         self.tile = int(tile)
@@ -217,16 +224,22 @@ class DeviceCase:
 
     def advance_from_host(self, Q_host: torch.Tensor, rhoi_host: torch.Tensor, nsteps: int,
                           Q_out: torch.Tensor, rhoi_out: torch.Tensor) -> None:
-        """End-to-end call with host buffers: uploads the primitive state (ghosted Q, rho_i,
-        ideally pinned), rebuilds U (prim2c, utils.jl:71-92), advances `nsteps` RK3 steps with
-        the fused stage and downloads the resulting Q, rho_i.  Asynchronous on the current
-        stream; synchronize before reading the outputs."""
-        if self.precision != 0:
-            raise abi.FlameError(5, "advance_from_host is implemented for the FP64 path")
+        """End-to-end call with host buffers: uploads the primitive state (ghosted Q, rho_i in
+        FP64, ideally pinned), rebuilds U (prim2c, utils.jl:71-92), advances `nsteps` RK3 steps
+        with the fused stage and downloads the resulting Q, rho_i (Q_out may be FP64 or the
+        storage type).  Asynchronous on the current stream; synchronize before reading."""
         Q, r = self.Q[self.cur], self.rhoi[self.cur]
-        Q.copy_(Q_host, non_blocking=True)
+        if self.precision == 0:
+            Q.copy_(Q_host, non_blocking=True)
+            q64 = Q
+        else:  # FP64 host state: U from the FP64 primitives, Q stored rounded to FP32
+            if getattr(self, "_q64", None) is None:
+                self._q64 = torch.empty(Q.shape, dtype=torch.float64, device=self.device)
+            q64 = self._q64
+            q64.copy_(Q_host, non_blocking=True)
+            Q.copy_(q64)
         r.copy_(rhoi_host, non_blocking=True)
-        self._call("flame_prim2c", _p(self.U), _p(Q))
+        self._call("flame_prim2c", _p(self.U), _p(q64))
         self._transport()
         for _ in range(nsteps):
             self.step()
