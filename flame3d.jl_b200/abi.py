@@ -108,6 +108,7 @@ SIGNATURES = {
     "flame_fillGhost": [G, S, P, P, P, P, TH, C.POINTER(FlameInflow), I, I],
     "flame_fillSpec": [G, S, P],
     "flame_cfl_max": [G, S, P, M, P],
+    "flame_check_finite": [G, S, P, I, P],
     "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
     "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],

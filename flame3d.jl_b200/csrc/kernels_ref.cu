@@ -535,6 +535,15 @@ __global__ void k_cfl_max(Dims D, const double *__restrict__ Q, FlameMetrics m,
     if ((threadIdx.x & 31) == 0 && bits) atomicMax(out, bits);
 }
 
+// Non-finite values of an array (solver.jl:388-391 tests isnan over U).
+__global__ void k_count_nonfinite(long long n, const double *__restrict__ A, unsigned int *count) {
+    unsigned int c = 0;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+        c += isfinite(A[i]) ? 0u : 1u;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 }  // namespace
 }  // namespace flame
 
@@ -791,6 +800,20 @@ int flame_fillGhost(const FlameGrid *g, flame_stream_t s, double *Q, double *U, 
 int flame_fillSpec(const FlameGrid *g, flame_stream_t s, double *rhoi) {
     if (int e = flame_fill_y_s(g, s, rhoi)) return e;
     return flame_fill_z_s(g, s, rhoi);
+}
+
+int flame_check_finite(const FlameGrid *g, flame_stream_t s, const double *A, int nv,
+                       unsigned int *count) {
+    if (int e = flame_check_grid(g, "flame_check_finite")) return e;
+    if (!A || !count || nv < 1) return flame_fail(FLAME_EINVAL, "flame_check_finite: bad argument");
+    const Dims D = make_dims(*g);
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess)
+        return flame_fail(FLAME_ELAUNCH, "flame_check_finite: %s", cudaGetErrorString(e));
+    const long long n = D.np * nv;
+    const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+    k_count_nonfinite<<<(unsigned)blocks, 256, 0, s>>>(n, A, count);
+    return flame_check_launch("flame_check_finite");
 }
 
 int flame_cfl_max(const FlameGrid *g, flame_stream_t s, const double *Q, const FlameMetrics *m,

@@ -271,6 +271,7 @@ class RequestRecord:
     first_step: float = math.nan
     finished: float = math.nan
     rejected: str | None = None
+    failed: str | None = None   # stopped early: the NaN check found a non-finite state
     finite: bool = True
     step_ms: list = field(default_factory=list, repr=False)
 
@@ -291,6 +292,7 @@ class _Slot:
     rec: RequestRecord
     dc: DeviceCase
     remaining: int
+    done_steps: int = 0
 
 
 class Server:
@@ -300,13 +302,16 @@ class Server:
     hbm_budget: bytes of resident case state admitted at once (resident_bytes per request).
     max_slots: cases advanced together at most.
     capture: replay a batch composition's step as CUDA graphs when that pays (_should_capture).
+    check_every: every that many steps each case's U is checked for NaN / inf (the reference's
+        check, solver.jl:388-391, every 10 steps); a failing case stops early, its result is
+        copied out for inspection and its slot and bytes are freed.
     keep_results: keep each finished case's (Q, rho_i) on the host in `results`.
     """
 
     def __init__(self, device="cuda", precision: int = 1, hbm_budget: float = 150e9,
                  max_slots: int = 64, streams: int = 16, capture: bool = True,
                  keep_results: bool = False, builder=build_request_case,
-                 capture_min_steps: int = 8, tile="auto"):
+                 capture_min_steps: int = 8, tile="auto", check_every: int = 10):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise abi.FlameError(1, "the server needs a CUDA device")
@@ -318,6 +323,7 @@ class Server:
         self.capture = capture
         self.capture_min_steps = capture_min_steps
         self.tile = tile
+        self.check_every = check_every
         self.keep_results = keep_results
         self.builder = builder
         self.results: dict[int, tuple[np.ndarray, np.ndarray]] = {}
@@ -369,7 +375,7 @@ class Server:
         jobs = []
         records: dict[int, RequestRecord] = {}
         st = {"used": 0, "busy_ms": 0.0, "build_s": 0.0, "download_s": 0.0, "capture_s": 0.0,
-              "rebuilds": 0, "captures": 0, "peak_active": 0, "peak_bytes": 0}
+              "rebuilds": 0, "captures": 0, "peak_active": 0, "peak_bytes": 0, "steps": 0}
         batch, stable, pending = None, 0, None
         step_ms: list[float] = []
         launch_s = 0.0  # host time of the last eager batch.step()
@@ -441,6 +447,14 @@ class Server:
                 if math.isnan(s.rec.first_step):
                     s.rec.first_step = now()
                 s.remaining -= 1
+                s.done_steps += 1
+            st["steps"] += 1
+            if self.check_every and st["steps"] % self.check_every == 0:
+                counts = [(s, s.dc.nonfinite_launch()) for s in active]
+                for s, c in counts:
+                    if s.remaining > 0 and int(c.item()) > 0:
+                        s.rec.failed = f"non-finite state after {s.done_steps} steps"
+                        s.remaining = 0
             done = [s for s in active if s.remaining == 0]
             if done:
                 ready = torch.cuda.Event()
@@ -486,7 +500,8 @@ class Server:
 
 def _report(records, step_ms, st) -> dict:
     busy_ms = st["busy_ms"]
-    done = [r for r in records.values() if r.rejected is None and not math.isnan(r.finished)]
+    done = [r for r in records.values()
+            if r.rejected is None and r.failed is None and not math.isnan(r.finished)]
     cs = sum(3 * r.steps * r.cells for r in done)
     first = min((r.arrival for r in records.values()), default=0.0)
     last = max((r.finished for r in done), default=first)
@@ -495,6 +510,7 @@ def _report(records, step_ms, st) -> dict:
     return {
         "requests": len(records), "completed": len(done),
         "rejected": sum(r.rejected is not None for r in records.values()),
+        "failed": sum(r.failed is not None for r in records.values()),
         "nonfinite": sum(not r.finite for r in done),
         "cell_stages": cs,
         "makespan_s": last - first,

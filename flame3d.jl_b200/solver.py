@@ -92,6 +92,20 @@ class DeviceCase:
         if sequence_buffers:
             self._alloc_sequence()
 
+    def nonfinite_launch(self) -> torch.Tensor:
+        """Queues flame_check_finite over U (solver.jl:388-391) and returns the device counter
+        it writes; read it after the stream has passed (`int(counter.item())`)."""
+        if getattr(self, "_nf", None) is None:
+            self._nf = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._call("flame_check_finite", _p(self.U), 5, _p(self._nf))
+        return self._nf
+
+    def check_finite(self) -> None:
+        """The reference's NaN check: raises FLAME_ENONFINITE when U holds NaN or inf."""
+        n = int(self.nonfinite_launch().item())
+        if n:
+            raise abi.FlameError(4, f"{self.case.name}: {n} non-finite conserved values")
+
     def restore_conserved(self, q64: torch.Tensor) -> None:
         """After the primitive state was replaced (a restart): U from the FP64 primitives
         (prim2c, utils.jl:71-92) and the transport of the state for the fused stage."""

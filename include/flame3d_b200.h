@@ -211,6 +211,13 @@ int flame_fillGhost(const FlameGrid *g, flame_stream_t stream, double *Q, double
 /* boundary.jl:188-191  fillSpec: fill_y_s, fill_z_s. */
 int flame_fillSpec(const FlameGrid *g, flame_stream_t stream, double *rhoi);
 
+/* solver.jl:388-391  `any(isnan, U)` every 10 steps, as a count: writes to the device unsigned
+ * *count how many of the nv ghosted FP64 fields' values are NaN or infinite (the reference
+ * tests NaN only; an infinity is as fatal).  The caller reads it and stops the case, the
+ * reference's "Oops, NaN detected" (FLAME_ENONFINITE on the host side). */
+int flame_check_finite(const FlameGrid *g, flame_stream_t stream, const double *A, int nv,
+                       unsigned int *count);
+
 /* Largest per-cell CFL rate max over interior cells of Σ_d J (|m_d·u| + c |m_d|), with m_d the
  * stored metric rows (dξ/dx … scaled by 1/J), c = sqrt(γ p / ρ) and γ = p/e + 1 (split.jl:40-41),
  * written to the device double *out (a stable time step is dt = CFL / *out).  New: the reference
