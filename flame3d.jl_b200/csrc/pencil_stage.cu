@@ -82,6 +82,11 @@ constexpr size_t smem_bytes() {
     return sizeof(CT) * Slots<NS>::N * 32 * WPB;
 }
 
+// Asks L2 for the line holding p ahead of its use (no register is held meanwhile).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ int clampi(int v, int lo, int hi) {
     return v < lo ? lo : (v > hi ? hi : v);
 }
@@ -428,6 +433,22 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
     const int a = seg * OWN - 3 + lane;
     const int gx = clampi(a + A.ng, 0, A.nx + 2 * A.ng - 1), gy = y + A.ng, gz = z + A.ng;
     const int g = gx + A.sy * gy + A.sz * gz;
+    if (lane >= 3 && lane < 3 + OWN && a < A.nx) {  // what the end of this sweep reads
+#pragma unroll
+        for (int n = 0; n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
+        if constexpr (FIN) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) {
+                prefetch_l2(A.U + g + n * A.np);
+                if (A.stage > 1) prefetch_l2(A.Un + g + n * A.np);
+            }
+#pragma unroll
+            for (int n = 0; n < NS; ++n) {
+                prefetch_l2(A.ri + g + n * A.np);
+                if (A.stage > 1) prefetch_l2(A.rn + g + n * A.np);
+            }
+        }
+    }
     point_phase<0, NS, QT, CT>(A, S, lane, g);
     __syncwarp();
     CT G[5 + NS];
@@ -473,11 +494,20 @@ __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT>
 }
 
 // Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
-// use whole 128-byte lines; 8 when the column slots would not fit in shared memory.
+// use whole 128-byte lines; 8 when the column slots would not fit in shared memory.  (Sizing
+// for two blocks per SM instead, 16/8/4 columns under 112 KB, measured 0-2 % faster with few
+// species and 6 % slower with nine.)  Host and device use this rule: the batch planner sizes
+// its work list with it.
+constexpr int slots_of(int ns) { return 37 + 5 * ns; }
+constexpr int staged_cols(int ns, size_t csz) {
+    return csz * slots_of(ns) * 33 * 16 <= 200 * 1024 ? 16 : 8;
+}
+
 template <int NS, typename CT>
 struct Staged {
-    static constexpr int COLS = (sizeof(CT) * Slots<NS>::N * 33 * 16 <= 200 * 1024) ? 16 : 8;
+    static_assert(Slots<NS>::N == slots_of(NS), "slots_of must follow Slots");
     static constexpr int STRIDE = Slots<NS>::N * 32 + 1;  // padded column region (bank spread)
+    static constexpr int COLS = staged_cols(NS, sizeof(CT));
 };
 
 // y or z sweep (DIR 1, 2).  The block stages the points of COLS neighbouring pencils with
@@ -499,6 +529,17 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     const int seg = bid % nseg, c2 = bid / nseg;
     if (c2 >= n_c2) return;
     const int tid = threadIdx.x;
+    if constexpr (PASS == 1) {  // the R this thread adds to in phase C: start fetching it now
+        const int cx = tid % COLS, l = tid / COLS;
+        const int x = xb * COLS + cx, ac = seg * OWN - 3 + l;
+        if (l >= 3 && l < 3 + OWN && ac < n_along && x < A.nx) {
+            const int gy = DIR == 1 ? ac + A.ng : c2 + A.ng;
+            const int gz = DIR == 1 ? c2 + A.ng : ac + A.ng;
+            const int g = (x + A.ng) + A.sy * gy + A.sz * gz;
+#pragma unroll
+            for (int n = 0; n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
+        }
+    }
     // ---- phase A, x-fastest: thread -> (column cx, pencil position l)
     {
         const int cx = tid % COLS, l = tid / COLS;
@@ -754,11 +795,7 @@ size_t args_size() { return sizeof(Args<QT>); }
 inline void case_items(const FlameGrid &g, int ns, int precision, int items[4]) {
     const int tx = g.nx + 2 * g.ng, ty = g.ny + 2 * g.ng, tz = g.nz + 2 * g.ng;
     const int np = tx * ty * tz;
-    int cols = 16;
-    // Staged<NS, CT>::COLS, evaluated on the host for the case's species count
-    const int nslot = 10 + 2 * ns + 4 + 10 + 3 + 1 + ns + 8 + 2 * ns + 1;
-    const size_t csz = precision == 0 ? 8 : 4;
-    if (csz * nslot * 33 * 16 > 200 * 1024) cols = 8;
+    const int cols = staged_cols(ns, precision == 0 ? 8 : 4);  // Staged<NS, CT>::COLS
     const int nxb = (g.nx + cols - 1) / cols;
     items[0] = (np + 255) / 256;
     items[1] = nxb * ((g.nz + OWN - 1) / OWN) * g.ny;  // z sweep
