@@ -377,12 +377,17 @@ def run_serve(args, f3d) -> int:
     time.sleep(0.3)
     base = S.fifo(reqs, dev, precision=0)
     torch.cuda.empty_cache()
+    seq = S.fifo(reqs, dev, precision=0, fused=False) if args.serve_sequence else None
+    torch.cuda.empty_cache()
     srv = S.Server(dev, precision=1, hbm_budget=150e9)
     rep = srv.run(reqs)
     clocks = clk.stop()
     if args.serve_log:
         with open(args.serve_log, "w") as fh:
-            for arm, r in (("fifo_fp64", base), ("serving_mixed", rep)):
+            for arm, r in (("fifo_fp64", base), ("fifo_fp64_sequence", seq),
+                           ("serving_mixed", rep)):
+                if r is None:
+                    continue
                 for pr in r["per_request"]:
                     fh.write(json.dumps({"arm": arm, **pr}) + "\n")
     drop = ("per_request",)
@@ -405,6 +410,8 @@ def run_serve(args, f3d) -> int:
            "completion_latency_s": rep["completion_latency_s"],
            "serving": summ(rep), "plain_fp64_fifo": summ(base),
            "speedup_vs_plain_fp64_fifo": value / base["mcell_stage_per_s"],
+           "plain_fp64_launch_sequence_fifo": summ(seq) if seq else None,
+           "speedup_vs_launch_sequence_fifo": (value / seq["mcell_stage_per_s"]) if seq else None,
            "clocks": clocks}
     print(json.dumps(out), flush=True)
     return 0
@@ -447,6 +454,8 @@ def main() -> int:
     ap.add_argument("--step-scale", type=float, default=0.05,
                     help="serve: factor on the requested 200-2000 steps")
     ap.add_argument("--serve-log", default=None, help="serve: per-request JSON lines to this file")
+    ap.add_argument("--serve-sequence", action="store_true",
+                    help="serve: also time the 1:1 launch-sequence FIFO (about a minute more)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="precision: RK3 steps before the errors are measured")
     args = ap.parse_args()

@@ -553,9 +553,11 @@ def pretune(requests: list[SolveRequest], device="cuda", precisions=(0, 1),
 
 
 def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
-         keep_results: bool = False, builder=build_request_case, tile="auto") -> dict:
+         keep_results: bool = False, builder=build_request_case, tile="auto",
+         fused: bool = True) -> dict:
     """The baseline: one case at a time in arrival order (plain stage launches, no batching,
-    no graphs), same arrival times, same GPU, same report."""
+    no graphs), same arrival times, same GPU, same report.  fused=False runs each stage as the
+    reference's own launch sequence of 1:1 kernels (the literal drop-in; FP64 only)."""
     dev = torch.device(device)
     main = torch.cuda.current_stream(dev)
     t0 = time.perf_counter()
@@ -572,7 +574,8 @@ def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
         rec.admitted = now()
         tb = time.perf_counter()
         case = builder(r, dev)
-        dc = DeviceCase(case, dev, precision=precision, tile=tile)
+        dc = DeviceCase(case, dev, precision=precision, tile=tile if fused else 3,
+                        sequence_buffers=not fused)
         case.Q = case.rhoi = None
         case.metrics = {}
         rec.name = case.name
@@ -582,7 +585,7 @@ def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
         for _ in range(r.steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(main)
-            dc.step()
+            dc.step(fused)
             e1.record(main)
             evs.append((e0, e1))
         main.synchronize()
