@@ -62,7 +62,8 @@ class FlameMetrics(C.Structure):
 
 class FlameStageBuffers(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("U", "Un", "Q_in", "Q_out", "rhoi_in", "rhoi_out",
-                                          "rhon", "trans_in", "trans_out", "scratch")]
+                                          "rhon", "trans_in", "trans_out", "scratch",
+                                          "metrics_lo")]
 
 
 class FlameCaseDesc(C.Structure):

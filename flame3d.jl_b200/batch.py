@@ -60,7 +60,8 @@ class Batch:
             d.dt = dc.dt
             d.buf = FlameStageBuffers(_p(dc.U), _p(dc.Un), _p(dc.Q[i]), _p(dc.Q[o]),
                                       _p(dc.rhoi[i]), _p(dc.rhoi[o]), _p(dc.rhon),
-                                      _p(dc.T[i]), _p(dc.T[o]), _p(dc.scratch))
+                                      _p(dc.T[i]), _p(dc.T[o]), _p(dc.scratch),
+                                      _p(dc.metrics_lo))
             d.metrics = dc.cmetrics
             d.thermo = dc.thermo
             d.transport = dc.transport

@@ -52,6 +52,7 @@ struct Args {
     const double *ri;
     double *ro, *rn;
     const double *met[10];
+    const QT *metq;  // the metrics rounded to QT once (mixed precision), or null
     QT *aux;     // ϕ (1) and Y (NS), ghosted
     double *R;   // right-hand side accumulator (5 + NS), ghosted indexing
     FlameThermo th;
@@ -169,8 +170,15 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 #define SV(slot) S[(slot) * 32 + l]
     const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]),
              p = CT(Q[g + 4 * np]), T = CT(Q[g + 5 * np]), ei = CT(Q[g + 6 * np]);
-    const CT A1 = ldg<CT>(A.met[3 * DIR], g), A2 = ldg<CT>(A.met[3 * DIR + 1], g),
-             A3 = ldg<CT>(A.met[3 * DIR + 2], g);
+    CT mv[10];
+    if (A.metq) {  // once-rounded copy: the same values without a conversion per load
+#pragma unroll
+        for (int m = 0; m < 10; ++m) mv[m] = CT(__ldg(A.metq + m * np + g));
+    } else {
+#pragma unroll
+        for (int m = 0; m < 10; ++m) mv[m] = ldg<CT>(A.met[m], g);
+    }
+    const CT A1 = mv[3 * DIR], A2 = mv[3 * DIR + 1], A3 = mv[3 * DIR + 2];
     // Steger-Warming split, split.jl:17-89 (divisions folded into reciprocals)
     {
         const CT gam = p * (CT(1) / ei) + 1;
@@ -215,7 +223,7 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
     }
     SV(SL::Q4 + 0) = u, SV(SL::Q4 + 1) = v, SV(SL::Q4 + 2) = w, SV(SL::Q4 + 3) = T;
 #pragma unroll
-    for (int m = 0; m < 10; ++m) SV(SL::MET + m) = ldg<CT>(A.met[m], g);
+    for (int m = 0; m < 10; ++m) SV(SL::MET + m) = mv[m];
 #pragma unroll
     for (int m = 0; m < 3; ++m) SV(SL::TR + m) = CT(A.Ti[g + m * np]);
     SV(SL::RHO) = rho;
@@ -658,6 +666,7 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
     const double *mm[10] = {m.dxidx,   m.dxidy,   m.dxidz,   m.detadx, m.detady,
                             m.detadz,  m.dzetadx, m.dzetady, m.dzetadz, m.J};
     for (int i = 0; i < 10; ++i) A.met[i] = mm[i];
+    A.metq = sizeof(QT) == 4 ? static_cast<const QT *>(b.metrics_lo) : nullptr;
     // scratch: R (5 + NS doubles per point) first, then ϕ and Y (1 + NS of QT per point)
     A.R = static_cast<double *>(scratch);
     A.aux = reinterpret_cast<QT *>(A.R + (size_t)(5 + g.ns) * A.np);

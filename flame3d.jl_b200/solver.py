@@ -59,6 +59,9 @@ class DeviceCase:
 
         self.metrics = {k: up(case.metrics[k]) for k in METRIC_NAMES}
         self.cmetrics = FlameMetrics(**{k: v.data_ptr() for k, v in self.metrics.items()})
+        # mixed precision: the metrics rounded to FP32 once (FlameStageBuffers.metrics_lo)
+        self.metrics_lo = (torch.stack([self.metrics[k] for k in METRIC_NAMES]).float()
+                           .contiguous() if precision == 1 else None)
         shp = case.Q.shape[1:]
         ns = case.ns
         self.Q = [up(case.Q, qdt), torch.empty((7,) + shp, dtype=qdt, device=dev)]
@@ -128,7 +131,7 @@ class DeviceCase:
         them), optionally with another configuration."""
         c = DeviceCase.__new__(DeviceCase)
         for a in ("lib", "case", "device", "precision", "grid", "thermo", "transport", "dt",
-                  "metrics", "cmetrics", "cur", "poly"):
+                  "metrics", "cmetrics", "cur", "poly", "metrics_lo"):
             setattr(c, a, getattr(self, a))
         c.Q = [q.clone() for q in self.Q]
         c.rhoi = [r.clone() for r in self.rhoi]
@@ -211,7 +214,8 @@ class DeviceCase:
         i, o = self.cur, 1 - self.cur
         b = FlameStageBuffers(_p(self.U), _p(self.Un), _p(self.Q[i]), _p(self.Q[o]),
                               _p(self.rhoi[i]), _p(self.rhoi[o]), _p(self.rhon),
-                              _p(self.T[i]), _p(self.T[o]), _p(self.scratch))
+                              _p(self.T[i]), _p(self.T[o]), _p(self.scratch),
+                              _p(self.metrics_lo))
         rc = self.lib.flame_rk_stage_tiled(C.byref(self.grid), C.c_void_p(self.stream), stage,
                                            self.dt, C.byref(b), C.byref(self.cmetrics),
                                            C.byref(self.thermo), C.byref(self.transport),

@@ -263,6 +263,10 @@ typedef struct FlameStageBuffers {
     void *trans_out;       /* (…,3) μ, λ, D of the stage result */
     void *scratch;         /* flame_stage_scratch_bytes() bytes for configurations 3 and 4,
                               else unused (may be NULL); contents need not survive calls */
+    const void *metrics_lo; /* optional, precision 1 and configurations 3-4: the ten metric
+                               fields rounded once to float, back to back in FlameMetrics
+                               order (10 x ghosted points); NULL rounds them at every load.
+                               The FP64 metrics are still read for J in the RK3 update. */
 } FlameStageBuffers;
 
 /* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 storage of Q and transport, FP32
