@@ -242,8 +242,9 @@ def run_ensemble(args, f3d) -> int:
     tuned = [S.DeviceCase(c, device=dev, precision=1, tile="auto") for c in cases]
     k = max(args.steps // 10, 10)
     modes = {}
-    for mode, dcs in (("graph", tuned), ("graph_pencil", pencil), ("persistent", pencil)):
-        batch = B.Batch(dcs, device=dev, mode=mode.split("_")[0])
+    for mode, dcs, nst in (("graph", tuned, 16), ("graph_s32", tuned, 32),
+                           ("graph_pencil", pencil, 16), ("persistent", pencil, 16)):
+        batch = B.Batch(dcs, device=dev, mode=mode.split("_")[0], streams=nst)
         batch.capture()
         for _ in range(max(args.warmup, 3)):
             batch.step()
@@ -270,7 +271,7 @@ def run_ensemble(args, f3d) -> int:
                       "tuned_configs": {str(t): sum(d.tile == t for d in tuned)
                                         for t in sorted({d.tile for d in tuned})},
                       "launches_per_step": (3 * sum(d.launches_per_stage() for d in tuned)
-                                            if best == "graph" else
+                                            if best in ("graph", "graph_s32") else
                                             3 * sum(d.launches_per_stage() for d in pencil)
                                             if best == "graph_pencil" else
                                             3 * 4 * len({c.ns for c in cases}))},
