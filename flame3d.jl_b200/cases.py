@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .abi import FLAME_MAX_NS, FLAME_NG, FlameGrid, FlameThermo, FlameTransport, METRIC_NAMES
+from .abi import FLAME_NG, FlameGrid, FlameThermo, FlameTransport, METRIC_NAMES
 
 RU = 8.314462618  # J/(mol K)
 NG = FLAME_NG

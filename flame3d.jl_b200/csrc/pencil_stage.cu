@@ -405,11 +405,15 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     // the cell and its periodic ghost images (new: the reference fills ghosts with case-specific
     // kernels, boundary.jl:1-191)
     const int ng = A.ng;
-    int ox[2] = {0, 0}, oy[2] = {0, 0}, oz[2] = {0, 0};
+    // up to two images per axis: an axis shorter than 2 NG has cells near both ends
+    int ox[3] = {0, 0, 0}, oy[3] = {0, 0, 0}, oz[3] = {0, 0, 0};
     int nxo = 1, nyo = 1, nzo = 1;
-    if (gx < 2 * ng) ox[nxo++] = A.nx; else if (gx >= A.nx) ox[nxo++] = -A.nx;
-    if (gy < 2 * ng) oy[nyo++] = A.ny; else if (gy >= A.ny) oy[nyo++] = -A.ny;
-    if (gz < 2 * ng) oz[nzo++] = A.nz; else if (gz >= A.nz) oz[nzo++] = -A.nz;
+    if (gx < 2 * ng) ox[nxo++] = A.nx;
+    if (gx >= A.nx) ox[nxo++] = -A.nx;
+    if (gy < 2 * ng) oy[nyo++] = A.ny;
+    if (gy >= A.ny) oy[nyo++] = -A.ny;
+    if (gz < 2 * ng) oz[nzo++] = A.nz;
+    if (gz >= A.nz) oz[nzo++] = -A.nz;
     for (int c = 0; c < nzo; ++c)
         for (int b = 0; b < nyo; ++b)
             for (int aa = 0; aa < nxo; ++aa) {

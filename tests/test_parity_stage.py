@@ -150,3 +150,26 @@ def test_autotuned_case_matches_fixed_configuration(f3d, cuda_ok, tmp_path, monk
     for n in range(5):
         scale = mom if 1 <= n <= 3 else np.linalg.norm(Uf[n].ravel())
         assert np.linalg.norm((Ua[n] - Uf[n]).ravel()) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("n", [6, 7, 27, 31])
+@pytest.mark.parametrize("tile", [0, 3, 4])
+def test_fused_odd_extents(f3d, oracle, cuda_ok, n, tile):
+    """Extents that divide neither the pencil (26 owned cells), the 16-column blocks nor the
+    tiles, down to 4 cells on an axis (random_curvilinear uses n+4, n, n-2)."""
+    S = f3d.solver_module()
+    case = f3d.random_curvilinear(n=n, ns=2, seed=90 + n)
+    dc = S.DeviceCase(case, tile=tile)
+    oc = oracle.OracleCase(case)
+    for s in (1, 2, 3):
+        dc.stage_fused(s)
+        oc.stage(s)
+    U = dc.conserved()
+    I = oracle.interior
+    mom = np.linalg.norm(I(oc.U[1:4]).ravel())
+    for k in range(5):
+        ref = I(oc.U[k])
+        scale = mom if 1 <= k <= 3 else np.linalg.norm(ref.ravel())
+        assert np.linalg.norm((I(U[k]) - ref).ravel()) <= 1e-12 * scale, (n, tile, k)
+    Q, r = dc.primitives()
+    assert np.array_equal(Q[:, :, :, :4], Q[:, :, :, case.nx:case.nx + 4])  # periodic ghosts
