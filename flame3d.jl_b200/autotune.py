@@ -2,7 +2,8 @@
 
 Configurations (flame_rk_stage_tiled): 0, 1, 2 = one tile kernel per stage (16x8x8 with one or
 two CTAs per SM, 8x8x8); 3 = prep + z, y, x pencil sweeps, the x sweep finishing the stage;
-4 = the same sweeps with the finish in its own per-cell launch.  Which is fastest depends on
+4 = the same sweeps with the finish in its own per-cell launch; 5, 6 = 3, 4 with each y / z
+sweep split into a flow sweep and a species sweep.  Which is fastest depends on
 the species count (registers and shared memory per point grow with it), on the grid size (the
 tile kernels launch once per stage, which matters for small grids) and on the precision.
 
@@ -20,7 +21,7 @@ import os
 import threading
 from pathlib import Path
 
-CANDIDATES = (0, 1, 2, 3, 4)
+CANDIDATES = (0, 1, 2, 3, 4, 5, 6)
 
 
 def cache_path() -> Path:

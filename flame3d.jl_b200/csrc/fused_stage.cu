@@ -28,7 +28,8 @@
 
 int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
                        const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *th,
-                       const FlameTransport *tr, int precision, void *scratch, int split_finish);
+                       const FlameTransport *tr, int precision, void *scratch, int split_finish,
+                       int split_species);
 
 namespace flame {
 namespace fused {
@@ -627,8 +628,11 @@ int dispatch_tile(int tile, int ns, const FlameGrid &g, cudaStream_t s, int stag
         case 2: return dispatch_ns<Cfg8x8x8, QT, CT>(ns, g, s, stage, dt, b, m, th, tr);
         case 3:
         case 4:
+        case 5:
+        case 6:
             return flame_pencil_stage(&g, s, stage, dt, &b, &m, &th, &tr,
-                                      sizeof(QT) == 8 ? 0 : 1, b.scratch, tile == 4);
+                                      sizeof(QT) == 8 ? 0 : 1, b.scratch, tile == 4 || tile == 6,
+                                      tile >= 5);
         default: return flame_fail(FLAME_EINVAL, "flame_rk_stage: tile config %d unknown", tile);
     }
 }

@@ -21,6 +21,7 @@
 // arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
 
 #include <cstring>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -76,7 +77,32 @@ struct Slots {
     static constexpr int PHI = DY2 + NS;
     static constexpr int N = PHI + 1;
     static constexpr int G = FP;                // face flux, reuses the split slots (5 + NS)
+    static constexpr int SPP = 10, SPM = 10 + NS;  // F+ / F- of species 0
+    static constexpr int D = TR + 2, T = Q4 + 3;
 };
+
+// Slots of the species sweep (PART 2): only what the species fluxes and the enthalpy
+// diffusion term of the energy flux read.
+template <int NS>
+struct SpSlots {
+    static constexpr int FP = 0;                // F+ sp (NS), F- sp (NS)
+    static constexpr int SPP = 0, SPM = NS;
+    static constexpr int MET = 2 * NS;          // 9 metrics + J
+    static constexpr int D = MET + 10;
+    static constexpr int RHO = D + 1;
+    static constexpr int T = RHO + 1;
+    static constexpr int PHI = T + 1;
+    static constexpr int Y = PHI + 1;           // NS
+    static constexpr int DY1 = Y + NS;          // NS
+    static constexpr int DY2 = DY1 + NS;        // NS
+    static constexpr int N = DY2 + NS;          // 5 NS + 14
+    static constexpr int G = FP;                // NS species fluxes + the energy term
+};
+
+// PART 0: the whole face flux; PART 2: the species fluxes and the enthalpy-diffusion term of the
+// energy flux only (the flow part then runs as the NS = 0 instance of the same sweep).
+template <int NS, int PART>
+using SlotsOf = std::conditional_t<PART == 2, SpSlots<NS>, Slots<NS>>;
 
 template <int NS, typename CT, int WPB>
 constexpr size_t smem_bytes() {
@@ -251,9 +277,10 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 // The species part runs one species at a time in two passes (the sums of the diffusion
 // velocities first, then each species' reconstruction, corrected diffusion flux and enthalpy
 // flux), recomputing the few gradient terms instead of holding per-species arrays in registers.
-template <int DIR, int NS, typename QT, typename CT>
+template <int DIR, int NS, typename QT, typename CT, int PART = 0>
 __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G) {
-    using SL = Slots<NS>;
+    using SL = SlotsOf<NS, PART>;
+    constexpr int GS = PART == 2 ? 0 : 5;  // G index of species 0
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
     const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
 #define SV(slot, ll) S[(slot) * 32 + (ll)]
@@ -266,17 +293,17 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
         pv[6] = mv[6] = CT(0);
         return hybrid_face_fast<CT>(pv, mv, phif);
     };
+    if constexpr (PART != 2) {
 #pragma unroll
-    for (int n = 0; n < 5; ++n) G[n] = recon(n, 5 + n);
+        for (int n = 0; n < 5; ++n) G[n] = recon(n, 5 + n);
+    }
     CT met[9];
 #pragma unroll
     for (int m = 0; m < 9; ++m) met[m] = (SV(SL::MET + m, lm) + SV(SL::MET + m, l)) * h;
     const CT Jac = (SV(SL::MET + 9, lm) + SV(SL::MET + 9, l)) * h;
-    const CT mui = (SV(SL::TR, lm) + SV(SL::TR, l)) * h;
-    const CT lami = (SV(SL::TR + 1, lm) + SV(SL::TR + 1, l)) * h;
-    const CT DL = SV(SL::TR + 2, lm), DR = SV(SL::TR + 2, l);
+    const CT DL = SV(SL::D, lm), DR = SV(SL::D, l);
     const CT rho = (SV(SL::RHO, lm) + SV(SL::RHO, l)) * h;
-    const CT Tf = (SV(SL::Q4 + 3, lm) + SV(SL::Q4 + 3, l)) * h;
+    const CT Tf = (SV(SL::T, lm) + SV(SL::T, l)) * h;
     const CT *md = met + 3 * DIR;
     // species diffusion (viscous.jl:430-507): the diffusion velocity of species n at the face
     const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
@@ -309,10 +336,15 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
             const CT Yf = diffusion(n, Vx, Vy, Vz);
             const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
             const CT V1 = Vx - sum1 * Yf, V2 = Vy - sum2 * Yf, V3 = Vz - sum3 * Yf;
-            G[5 + n] = recon(10 + n, 10 + NS + n) - (V1 * md[0] + V2 * md[1] + V3 * md[2]);
+            G[GS + n] = recon(SL::SPP + n, SL::SPM + n) - (V1 * md[0] + V2 * md[1] + V3 * md[2]);
             fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
         }
     }
+    if constexpr (PART == 2) {  // the energy flux's enthalpy-diffusion term, viscous.jl:120-141
+        G[NS] = -(md[0] * fh1 + md[1] * fh2 + md[2] * fh3);
+    } else {
+    const CT mui = (SV(SL::TR, lm) + SV(SL::TR, l)) * h;
+    const CT lami = (SV(SL::TR + 1, lm) + SV(SL::TR + 1, l)) * h;
     // momentum and energy, viscous.jl:14-141
     CT gr[4][3];
 #pragma unroll
@@ -344,6 +376,52 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
     G[2] -= md[0] * t12 + md[1] * t22 + md[2] * t23;
     G[3] -= md[0] * t13 + md[1] * t23 + md[2] * t33;
     G[4] -= md[0] * E1 + md[1] * E2 + md[2] * E3;
+    }
+}
+
+// ---- phase A of the species sweep: the species slots of one point.
+template <int DIR, int NS, typename QT, typename CT>
+__device__ __forceinline__ void species_point_phase(const Args<QT> &A, CT *S, int l, int g) {
+    using SL = SpSlots<NS>;
+    constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
+    const int np = A.np;
+    const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
+    const int s2 = D2 == 0 ? 1 : (D2 == 1 ? A.sy : A.sz);
+    const QT *Q = A.Qi;
+    const CT h = CT(0.5);
+#define SV(slot) S[(slot) * 32 + l]
+    const CT rho = CT(Q[g]), u = CT(Q[g + np]), v = CT(Q[g + 2 * np]), w = CT(Q[g + 3 * np]);
+    CT mv[10];
+    if (A.metq) {
+#pragma unroll
+        for (int m = 0; m < 10; ++m) mv[m] = CT(__ldg(A.metq + m * np + g));
+    } else {
+#pragma unroll
+        for (int m = 0; m < 10; ++m) mv[m] = ldg<CT>(A.met[m], g);
+    }
+    // species split, split.jl:101-130 (the contravariant velocity as in point_phase)
+    const CT E1 = mv[3 * DIR] * u + mv[3 * DIR + 1] * v + mv[3 * DIR + 2] * w;
+    const CT Ep = h * (E1 + fabs(E1)), Em = h * (E1 - fabs(E1));
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        const CT r = CT(A.ri[g + n * np]);
+        SV(SL::SPP + n) = Ep * r;
+        SV(SL::SPM + n) = Em * r;
+    }
+#pragma unroll
+    for (int m = 0; m < 10; ++m) SV(SL::MET + m) = mv[m];
+    SV(SL::D) = CT(A.Ti[g + 2 * np]);
+    SV(SL::RHO) = rho;
+    SV(SL::T) = CT(Q[g + 5 * np]);
+    SV(SL::PHI) = CT(A.aux[g]);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        const QT *Y = A.aux + (1 + n) * np;
+        SV(SL::Y + n) = CT(Y[g]);
+        SV(SL::DY1 + n) = CT(Y[g + s1]) - CT(Y[g - s1]);
+        SV(SL::DY2 + n) = CT(Y[g + s2]) - CT(Y[g - s2]);
+    }
+#undef SV
 }
 
 // ---- last sweep: div, RK3 combination, c2Prim, transport, ghost images of one cell.
@@ -515,21 +593,27 @@ constexpr int staged_cols(int ns, size_t csz) {
     return csz * slots_of(ns) * 33 * 16 <= 200 * 1024 ? 16 : 8;
 }
 
-template <int NS, typename CT>
+template <int NS, typename CT, int PART = 0>
 struct Staged {
     static_assert(Slots<NS>::N == slots_of(NS), "slots_of must follow Slots");
-    static constexpr int STRIDE = Slots<NS>::N * 32 + 1;  // padded column region (bank spread)
-    static constexpr int COLS = staged_cols(NS, sizeof(CT));
+    static constexpr int NSLOT = SlotsOf<NS, PART>::N;
+    static constexpr int STRIDE = NSLOT * 32 + 1;  // padded column region (bank spread)
+    // (the species sweep in 8-column blocks capped at three per SM measured 7-12 % slower in
+    // mixed precision: the register cap spills)
+    static constexpr int COLS =
+        PART == 2 ? (sizeof(CT) * NSLOT * 33 * 16 <= 200 * 1024 ? 16 : 8)
+                  : staged_cols(NS, sizeof(CT));
 };
 
 // y or z sweep (DIR 1, 2).  The block stages the points of COLS neighbouring pencils with
 // x-fastest threads (coalesced loads), then each warp works its own pencil from shared memory
 // exactly like the x sweep, and the right-hand side goes back with x-fastest threads.
 // PASS 0 writes R, PASS 1 adds to it.
-template <int DIR, int PASS, int NS, typename QT, typename CT>
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
 __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsigned char *smem_raw) {
-    constexpr int COLS = Staged<NS, CT>::COLS, STRIDE = Staged<NS, CT>::STRIDE;
-    using SL = Slots<NS>;
+    constexpr int COLS = Staged<NS, CT, PART>::COLS, STRIDE = Staged<NS, CT, PART>::STRIDE;
+    using SL = SlotsOf<NS, PART>;
+    constexpr int NG_OUT = PART == 2 ? NS + 1 : 5 + NS;  // face values a lane produces
     CT *base = reinterpret_cast<CT *>(smem_raw);
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
@@ -549,7 +633,7 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
             const int gz = DIR == 1 ? c2 + A.ng : ac + A.ng;
             const int g = (x + A.ng) + A.sy * gy + A.sz * gz;
 #pragma unroll
-            for (int n = 0; n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
+            for (int n = (PART == 2 ? 4 : 0); n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
         }
     }
     // ---- phase A, x-fastest: thread -> (column cx, pencil position l)
@@ -561,20 +645,23 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
         const int gx = x + A.ng;
         const int gy = DIR == 1 ? ga : c2 + A.ng;
         const int gz = DIR == 1 ? c2 + A.ng : ga;
-        point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
+        if constexpr (PART == 2)
+            species_point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
+        else
+            point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
     }
     __syncthreads();
     // ---- phase B, one warp per pencil (column)
     const int warp = tid >> 5, lane = tid & 31;
     CT *S = base + warp * STRIDE;
     const int a = seg * OWN - 3 + lane;
-    CT G[5 + NS];
+    CT G[NG_OUT];
     const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
-    if (face) face_phase<DIR, NS, QT, CT>(A, S, lane, G);
+    if (face) face_phase<DIR, NS, QT, CT, PART>(A, S, lane, G);
     __syncwarp();
     if (face) {
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) S[(SL::G + n) * 32 + lane] = G[n];
+        for (int n = 0; n < NG_OUT; ++n) S[(SL::G + n) * 32 + lane] = G[n];
     }
     __syncthreads();
     // ---- phase C, x-fastest again: cell differences into R
@@ -587,18 +674,21 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     const int g = (x + A.ng) + A.sy * gy + A.sz * gz;
     const CT *Sc = base + cx * STRIDE;
 #pragma unroll
-    for (int n = 0; n < 5 + NS; ++n) {
+    for (int n = 0; n < NG_OUT; ++n) {
         const double d = double(Sc[(SL::G + n) * 32 + l]) - double(Sc[(SL::G + n) * 32 + l + 1]);
-        if (PASS == 0) A.R[g + n * A.np] = d;
-        else A.R[g + n * A.np] += d;
+        // PART 2: G[n] is species n (R field 5 + n) and G[NS] the energy term (R field 4,
+        // written by the flow sweep of this direction just before)
+        const int f = PART == 2 ? (n < NS ? 5 + n : 4) : n;
+        if (PASS == 0 && !(PART == 2 && n == NS)) A.R[g + f * A.np] = d;
+        else A.R[g + f * A.np] += d;
     }
 }
 
-template <int DIR, int PASS, int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
+__global__ void __launch_bounds__(Staged<NS, CT, PART>::COLS * 32)
     k_pencil_staged(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    staged_block<DIR, PASS, NS, QT, CT>(A, blockIdx.x, smem_raw);
+    staged_block<DIR, PASS, NS, QT, CT, PART>(A, blockIdx.x, smem_raw);
 }
 
 // ---------------------------------------------------------------------- batched, persistent
@@ -691,17 +781,17 @@ int set_smem(K kernel, size_t sm, bool *done) {
     return FLAME_OK;
 }
 
-template <int DIR, int PASS, int NS, typename QT, typename CT>
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
 int launch_staged(const Args<QT> &A, cudaStream_t s) {
-    using ST = Staged<NS, CT>;
+    using ST = Staged<NS, CT, PART>;
     constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
     static bool done[64] = {};
-    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT>, sm, done)) return e;
+    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART>, sm, done)) return e;
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
     const long long blocks = (long long)((A.nx + ST::COLS - 1) / ST::COLS) *
                              ((n_along + OWN - 1) / OWN) * n_c2;
-    k_pencil_staged<DIR, PASS, NS, QT, CT><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    k_pencil_staged<DIR, PASS, NS, QT, CT, PART><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
@@ -719,12 +809,19 @@ int launch_x(const Args<QT> &A, cudaStream_t s) {
 template <int NS, typename QT, typename CT>
 int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const FlameStageBuffers &b,
            const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr,
-           void *scratch, bool split_finish) {
+           void *scratch, bool split_finish, bool split_species) {
     const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr, scratch);
     k_prep<NS, QT><<<(unsigned)((A.np + 255) / 256), 256, 0, s>>>(A);
     if (int e = flame_check_launch("flame_rk_stage (prep)")) return e;
-    if (int e = launch_staged<2, 0, NS, QT, CT>(A, s)) return e;
-    if (int e = launch_staged<1, 1, NS, QT, CT>(A, s)) return e;
+    if (split_species) {  // configurations 5, 6: flow sweep (the NS = 0 instance) + species sweep
+        if (int e = launch_staged<2, 0, 0, QT, CT>(A, s)) return e;
+        if (int e = launch_staged<2, 0, NS, QT, CT, 2>(A, s)) return e;
+        if (int e = launch_staged<1, 1, 0, QT, CT>(A, s)) return e;
+        if (int e = launch_staged<1, 1, NS, QT, CT, 2>(A, s)) return e;
+    } else {
+        if (int e = launch_staged<2, 0, NS, QT, CT>(A, s)) return e;
+        if (int e = launch_staged<1, 1, NS, QT, CT>(A, s)) return e;
+    }
     if (!split_finish) return launch_x<NS, QT, CT, true>(A, s);
     if (int e = launch_x<NS, QT, CT, false>(A, s)) return e;
     const long long cells = (long long)A.nx * A.ny * A.nz;
@@ -735,10 +832,10 @@ int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const Flame
 template <typename QT, typename CT>
 int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
              const FlameStageBuffers &b, const FlameMetrics &m, const FlameThermo &th,
-             const FlameTransport &tr, void *scratch, bool split_finish) {
+             const FlameTransport &tr, void *scratch, bool split_finish, bool split_species) {
     switch (ns) {
 #define CASE(N) \
-    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr, scratch, split_finish);
+    case N: return launch<N, QT, CT>(g, s, stage, dt, b, m, th, tr, scratch, split_finish, split_species);
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
         default:
@@ -753,16 +850,18 @@ int dispatch(int ns, const FlameGrid &g, cudaStream_t s, int stage, double dt,
 // Entry used by fused_stage.cu's dispatcher for tile configuration 3.
 int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
                        const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *th,
-                       const FlameTransport *tr, int precision, void *scratch, int split_finish) {
+                       const FlameTransport *tr, int precision, void *scratch, int split_finish,
+                       int split_species) {
     if (!scratch)
         return flame_fail(FLAME_EINVAL,
                           "flame_rk_stage: the pencil configuration needs scratch (see "
                           "flame_stage_scratch_bytes)");
     if (precision == 0)
         return flame::pencil::dispatch<double, double>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
-                                                       scratch, split_finish != 0);
+                                                       scratch, split_finish != 0,
+                                                       split_species != 0);
     return flame::pencil::dispatch<float, float>(g->ns, *g, s, stage, dt, *b, *m, *th, *tr,
-                                                 scratch, split_finish != 0);
+                                                 scratch, split_finish != 0, split_species != 0);
 }
 
 extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {

@@ -119,7 +119,7 @@ class DeviceCase:
     def set_tile(self, tile: int) -> None:
         """Switches the fused stage's configuration (the pencil ones need scratch)."""
         self.tile = int(tile)
-        if self.tile in (3, 4):
+        if self.tile in (3, 4, 5, 6):
             if self.scratch is None:
                 nbytes = self.lib.flame_stage_scratch_bytes(C.byref(self.grid), self.precision)
                 self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
@@ -224,16 +224,18 @@ class DeviceCase:
         self.cur = o
 
     def launches_per_stage(self) -> int:
-        """Kernels one fused stage launches: 4 (5 with the separate finish) for the pencil
-        sweeps, 1 for a tile kernel."""
-        return {3: 4, 4: 5}.get(self.tile, 1)
+        """Kernels one fused stage launches: 4 for the pencil sweeps, one more with the
+        separate finish (4, 6) and two more with split species sweeps (5, 6); 1 for a tile
+        kernel."""
+        return {3: 4, 4: 5, 5: 6, 6: 7}.get(self.tile, 1)
 
     def stage_kernels(self) -> str:
-        if self.tile == 3:
-            return "pencil::k_prep + k_pencil_staged<z> + k_pencil_staged<y> + k_pencil_x"
-        if self.tile == 4:
-            return ("pencil::k_prep + k_pencil_staged<z> + k_pencil_staged<y> + k_pencil_x"
-                    " + k_finish")
+        if self.tile in (3, 4, 5, 6):
+            yz = ("k_pencil_staged<z> + k_pencil_staged<y>" if self.tile < 5 else
+                  "k_pencil_staged<z, flow> + k_pencil_staged<z, species> + "
+                  "k_pencil_staged<y, flow> + k_pencil_staged<y, species>")
+            fin = " + k_finish" if self.tile in (4, 6) else ""
+            return f"pencil::k_prep + {yz} + k_pencil_x{fin}"
         return "fused::k_stage<tile %d>" % self.tile
 
     def step(self, fused: bool = True) -> None:

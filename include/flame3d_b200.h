@@ -261,7 +261,7 @@ typedef struct FlameStageBuffers {
     double *rhon;          /* (…,ns) RK3 stage-0 copy */
     const void *trans_in;  /* (…,3) μ, λ, D of the stage input */
     void *trans_out;       /* (…,3) μ, λ, D of the stage result */
-    void *scratch;         /* flame_stage_scratch_bytes() bytes for configurations 3 and 4,
+    void *scratch;         /* flame_stage_scratch_bytes() bytes for configurations 3 to 6,
                               else unused (may be NULL); contents need not survive calls */
     const void *metrics_lo; /* optional, precision 1 and configurations 3-4: the ten metric
                                fields rounded once to float, back to back in FlameMetrics
@@ -281,7 +281,9 @@ int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double 
  * with one CTA per SM, 16x8x8 with two, 8x8x8 with two); 3 = four barrier-free launches
  * (a prep pass and z, y, x warp-per-pencil sweeps, the x sweep finishing the stage) that need
  * b->scratch; 4 = configuration 3 with the finish (RK3 update, c2Prim, transport, ghosts) in a
- * fifth, per-cell launch, bit-identical to 3.  The autotuner picks the configuration per grid,
+ * fifth, per-cell launch, bit-identical to 3; 5, 6 = configurations 3, 4 with each y / z sweep
+ * split into a flow sweep and a species sweep (fewer registers and shared-memory slots per
+ * sweep when there are many species).  The autotuner picks the configuration per grid,
  * species count and precision. */
 int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                          const FlameStageBuffers *b, const FlameMetrics *m,

@@ -63,7 +63,7 @@ def test_sequence_matches_oracle(f3d, oracle, cuda_ok, name):
     assert max(e.values()) <= 1e-14, e
 
 
-TILES = [0, 1, 2, 3, 4]
+TILES = [0, 1, 2, 3, 4, 5, 6]
 
 
 @pytest.mark.parametrize("tile", TILES)
@@ -153,7 +153,7 @@ def test_autotuned_case_matches_fixed_configuration(f3d, cuda_ok, tmp_path, monk
 
 
 @pytest.mark.parametrize("n", [6, 7, 27, 31])
-@pytest.mark.parametrize("tile", [0, 3, 4])
+@pytest.mark.parametrize("tile", [0, 3, 4, 5])
 def test_fused_odd_extents(f3d, oracle, cuda_ok, n, tile):
     """Extents that divide neither the pencil (26 owned cells), the 16-column blocks nor the
     tiles, down to 4 cells on an axis (random_curvilinear uses n+4, n, n-2)."""
