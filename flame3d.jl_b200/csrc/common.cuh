@@ -8,6 +8,8 @@
 
 #include "../../include/flame3d_b200.h"
 
+#include <nvtx3/nvToolsExt.h>  // header-only; a no-op unless a profiler is attached
+
 namespace flame {
 
 constexpr double kEps = 2.220446049250313e-16;  // CUDA.eps(Float64), utils.jl:100
@@ -438,6 +440,14 @@ __device__ __forceinline__ void mixture_properties(double T, double P, const dou
         Dk[n * stride] = (1 - X[n]) / (s + kEps);
     }
 }
+
+// An NVTX range over a host-side scope (stage launches show up by name in Nsight timelines).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 }  // namespace flame
 

@@ -692,6 +692,8 @@ extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int st
                                     const FlameStageBuffers *b, const FlameMetrics *m,
                                     const FlameThermo *th, const FlameTransport *tr,
                                     int precision, int tile) {
+    static const char *kNames[3] = {"flame_rk_stage 1", "flame_rk_stage 2", "flame_rk_stage 3"};
+    flame::NvtxRange range(kNames[(stage >= 1 && stage <= 3) ? stage - 1 : 0]);
     if (int e = flame_check_grid(g, "flame_rk_stage")) return e;
     if (int e = check_sizes(g, "flame_rk_stage")) return e;
     if (!b || !m || !th || !tr || !b->U || !b->Un || !b->Q_in || !b->Q_out || !b->rhoi_in ||

@@ -1116,6 +1116,7 @@ extern "C" int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, 
 }
 
 extern "C" int flame_batch_stage(FlameBatch *B, flame_stream_t s, int stage, int parity) {
+    flame::NvtxRange range("flame_batch_stage");
     if (!B) return flame_fail(FLAME_EINVAL, "flame_batch_stage: NULL batch");
     if (stage < 1 || stage > 3 || (parity != 0 && parity != 1))
         return flame_fail(FLAME_EINVAL, "flame_batch_stage: stage=%d parity=%d", stage, parity);

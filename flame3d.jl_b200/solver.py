@@ -239,8 +239,10 @@ class DeviceCase:
         return "fused::k_stage<tile %d>" % self.tile
 
     def step(self, fused: bool = True) -> None:
+        torch.cuda.nvtx.range_push(f"step {self.case.name}")
         for s in (1, 2, 3):
             (self.stage_fused if fused else self.stage_sequence)(s)
+        torch.cuda.nvtx.range_pop()
 
     def advance_from_host(self, Q_host: torch.Tensor, rhoi_host: torch.Tensor, nsteps: int,
                           Q_out: torch.Tensor, rhoi_out: torch.Tensor) -> None:

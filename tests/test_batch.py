@@ -104,3 +104,24 @@ def test_batch_agrees_with_single_case_path(f3d, cuda_ok):
         n = np.linalg.norm(a.ravel())
         assert np.linalg.norm((a - c).ravel()) <= 1e-13 * n
     b.close()
+
+
+def test_graph_batch_with_mixed_configurations(f3d, cuda_ok):
+    """Autotuned cases each keep their own configuration inside one graph-mode batch; every
+    case ends bit for bit where it ends when run alone with that configuration."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)
+    tiles = [0, 3, 4, 5, 6]
+    batched = [S.DeviceCase(c, precision=1, tile=t) for c, t in zip(cases, tiles)]
+    alone = [S.DeviceCase(c, precision=1, tile=t) for c, t in zip(cases, tiles)]
+    b = B.Batch(batched, mode="graph")
+    b.capture()
+    for _ in range(2):
+        b.step()
+        for dc in alone:
+            dc.step()
+    for x, y in zip(batched, alone):
+        for a, c in zip(_state(x), _state(y)):
+            assert np.array_equal(a, c)
+    b.close()
