@@ -315,6 +315,48 @@ __device__ __forceinline__ float wenoz_combine_fast<float>(float s11, float s22,
     return (1.0f / 6.0f) * ((a1 * r) * v1 + (a2 * r) * v2 + (a3 * r) * v3);
 }
 
+// wenoz_combine_fast<double> as a fraction N / D (so two faces can share one division).
+__device__ __forceinline__ void wenoz_fraction(double s11, double s22, double s33, double v1,
+                                               double v2, double v3, double &N, double &D) {
+    const double b1 = kWenoEps + s11, b2 = kWenoEps + s22, b3 = kWenoEps + s33;
+    const double tau = fabs(s11 - s33);
+    const double t = tau * tau;
+    const double p1 = b1 * b1, p2 = b2 * b2, p3 = b3 * b3;
+    const double a1 = (p1 + t) * (p2 * p3);
+    const double a2 = 6.0 * (p2 + t) * (p1 * p3);
+    const double a3 = 3.0 * (p3 + t) * (p1 * p2);
+    N = a1 * v1 + a2 * v2 + a3 * v3;
+    D = 6.0 * (a1 + a2 + a3);
+}
+
+__device__ __forceinline__ void wenoz_plus_fraction(double V1, double V2, double V3, double V4,
+                                                    double V5, double &N, double &D) {
+    const double tmp1 = 13.0 / 12.0, q4 = 0.25;
+    double a, b;
+    a = V1 - 2 * V2 + V3, b = V1 - 4 * V2 + 3 * V3;
+    const double s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V2 - V4;
+    const double s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V4 + V5, b = 3 * V3 - 4 * V4 + V5;
+    const double s33 = tmp1 * (a * a) + q4 * (b * b);
+    wenoz_fraction(s11, s22, s33, 2 * V1 - 7 * V2 + 11 * V3, -V2 + 5 * V3 + 2 * V4,
+                   2 * V3 + 5 * V4 - V5, N, D);
+}
+
+__device__ __forceinline__ void wenoz_minus_fraction(double V1, double V2, double V3, double V4,
+                                                     double V5, double &N, double &D) {
+    const double tmp1 = 13.0 / 12.0, q4 = 0.25;
+    double a, b;
+    a = V5 - 2 * V4 + V3, b = V5 - 4 * V4 + 3 * V3;
+    const double s11 = tmp1 * (a * a) + q4 * (b * b);
+    a = V2 - 2 * V3 + V4, b = V4 - V2;
+    const double s22 = tmp1 * (a * a) + q4 * (b * b);
+    a = V3 - 2 * V2 + V1, b = 3 * V3 - 4 * V2 + V1;
+    const double s33 = tmp1 * (a * a) + q4 * (b * b);
+    wenoz_fraction(s11, s22, s33, 11 * V3 - 7 * V4 + 2 * V5, -V4 + 5 * V3 + 2 * V2,
+                   2 * V3 + 5 * V2 - V1, N, D);
+}
+
 template <typename T>
 __device__ __forceinline__ T wenoz_plus_fast(T V1, T V2, T V3, T V4, T V5) {
     const T tmp1 = T(13.0 / 12.0), q4 = T(0.25);
@@ -354,8 +396,19 @@ __device__ __forceinline__ T hybrid_face_fast(const T *p, const T *m, T phif) {
         fm = T(kUP7_7) * m[0] + T(kUP7_6) * m[1] + T(kUP7_5) * m[2] + T(kUP7_4) * m[3] +
              T(kUP7_3) * m[4] + T(kUP7_2) * m[5];
     } else if (phif < T(kHybrid2)) {
-        fp = wenoz_plus_fast(p[0], p[1], p[2], p[3], p[4]);
-        fm = wenoz_minus_fast(m[1], m[2], m[3], m[4], m[5]);
+        if constexpr (sizeof(T) == 8) {
+            // FP64: F+ and F- share one division, Np/Dp + Nm/Dm = (Np Dm + Nm Dp) / (Dp Dm),
+            // while the product of the denominators stays inside the normal range
+            double Np, Dp, Nm, Dm;
+            wenoz_plus_fraction(p[0], p[1], p[2], p[3], p[4], Np, Dp);
+            wenoz_minus_fraction(m[1], m[2], m[3], m[4], m[5], Nm, Dm);
+            const double den = Dp * Dm;
+            if (den > 1e-300 && den < 1e300) return (Np * Dm + Nm * Dp) / den;
+            return Np / Dp + Nm / Dm;
+        } else {
+            fp = wenoz_plus_fast(p[0], p[1], p[2], p[3], p[4]);
+            fm = wenoz_minus_fast(m[1], m[2], m[3], m[4], m[5]);
+        }
     } else {
         fp = p[2] + T(0.5) * minmod(p[3] - p[2], p[2] - p[1]);
         fm = m[3] - T(0.5) * minmod(m[4] - m[3], m[3] - m[2]);
