@@ -274,6 +274,36 @@ def test_viscous_flux_divergence_is_fourth_order(f3d, oracle):
     assert 12 < errs[0] / errs[1] < 20, errs
 
 
+def test_tgv_initial_viscous_dissipation(f3d, oracle):
+    """At t = 0 the viscous terms of the momentum equation take kinetic energy out of the
+    Taylor-Green vortex at the rate ε = μ ∫ ω² dV = (3/4) μ U0² (2π)³ (u = U0 sin x cos y cos z,
+    v = −U0 cos x sin y cos z, w = 0: ω² averages to 3 U0²/4).  The oracle's viscous momentum
+    right-hand side (one stage with μ minus one with μ = 0, which removes every inviscid term)
+    must converge to it.  The normal second derivatives are 4th order, but viscous.jl averages
+    the cell-centred tangential derivatives to the faces, so the cross terms of the stress, and
+    with them ε, converge at 2nd order (0.26 % at 16³, 0.070 % at 32³)."""
+    rates = []
+    for n in (16, 32):
+        case = f3d.taylor_green(n=n, Re=1600.0, Ma=0.1)
+        mu = case.transport.mu_ref
+        U0 = case.info["U0"]
+        dU = []
+        for m in (mu, 0.0):
+            case.transport = f3d.Transport(law=0, mu_ref=m, Pr=0.71, lambda_ref=0.0, D_ref=0.0)
+            oc = oracle.OracleCase(case)
+            U0s = oc.U.copy()
+            oc.stage(1)
+            dU.append((oc.U - U0s) / case.dt)
+        visc = oracle.interior(dU[0] - dU[1])      # d(ρu)/dt from the viscous stress alone
+        Q = oracle.interior(case.Q)
+        h = 2 * math.pi / n
+        eps = -np.sum(Q[1] * visc[1] + Q[2] * visc[2] + Q[3] * visc[3]) * h ** 3
+        exact = 0.75 * mu * U0 ** 2 * (2 * math.pi) ** 3
+        rates.append(abs(eps / exact - 1))
+    assert rates[1] < 1e-3, rates
+    assert 3.3 < rates[0] / rates[1] < 4.7, rates     # 2nd order
+
+
 def test_oracle_regression_fixture(f3d, oracle):
     """The oracle reproduces its frozen outputs on three seeded cases."""
     import sys
