@@ -323,9 +323,22 @@ def run_precision(args, f3d) -> int:
             res[prec] = (dc.conserved(), time.perf_counter() - t0)
             del dc
             torch.cuda.empty_cache()
-        out["full_size"][name] = {"mixed_vs_fp64": _conserved_errors(res[1][0], res[0][0], I),
-                                  "finite": bool(np.isfinite(res[1][0]).all()),
-                                  "seconds": {"fp64": res[0][1], "mixed": res[1][1]}}
+        entry = {"mixed_vs_fp64": _conserved_errors(res[1][0], res[0][0], I),
+                 "finite": bool(np.isfinite(res[1][0]).all()),
+                 "seconds": {"fp64": res[0][1], "mixed": res[1][1]}}
+        if name.startswith("jet"):
+            # the flow's own sensitivity: plain FP64 from the initial state rounded to FP32
+            import copy
+            rounded = copy.copy(case)
+            rounded.Q = case.Q.astype(np.float32).astype(np.float64)
+            dc = S.DeviceCase(rounded, device=dev, precision=0, tile=3)
+            for _ in range(steps):
+                dc.step()
+            entry["fp64_from_fp32_rounded_start_vs_fp64"] = _conserved_errors(
+                dc.conserved(), res[0][0], I)
+            del dc
+            torch.cuda.empty_cache()
+        out["full_size"][name] = entry
         print(json.dumps({name: out["full_size"][name]}), flush=True)
     small = [("tgv32", f3d.taylor_green(n=32)),
              ("jet64x32x32", f3d.curvilinear_jet(nx=64, ny=32, nz=32)),
