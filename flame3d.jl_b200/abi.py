@@ -56,6 +56,13 @@ class FlameInflow(C.Structure):
                 ("w", C.c_double), ("Y", C.c_double * FLAME_MAX_NS)]
 
 
+class FlameReactions(C.Structure):
+    _fields_ = [("nreacs", C.c_int32), ("pad", C.c_int32), ("atm", C.c_double),
+                ("reaction_type", C.c_void_p), ("sgm", C.c_void_p), ("vf", C.c_void_p),
+                ("vr", C.c_void_p), ("Arr", C.c_void_p), ("ef", C.c_void_p), ("loP", C.c_void_p),
+                ("Troe", C.c_void_p)]
+
+
 class FlameMetrics(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in METRIC_NAMES]
 
@@ -110,6 +117,8 @@ SIGNATURES = {
     "flame_fillSpec": [G, S, P],
     "flame_cfl_max": [G, S, P, M, P],
     "flame_check_finite": [G, S, P, I, P],
+    "flame_eval_gpu": [G, S, P, P, P, D, TH, C.POINTER(FlameReactions), P, D],
+    "flame_eval_gpu_stiff": [G, S, P, P, P, D, TH, C.POINTER(FlameReactions), P, D, I],
     "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
     "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],

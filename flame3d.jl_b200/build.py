@@ -29,6 +29,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # evaluation of the reference arithmetic bit for bit.  The fused kernels let ptxas contract.
 PER_FILE = {
     "kernels_ref.cu": ["-fmad=false"],
+    "chemistry.cu": ["-fmad=false"],
 }
 
 

@@ -211,6 +211,38 @@ int flame_fillGhost(const FlameGrid *g, flame_stream_t stream, double *Q, double
 /* boundary.jl:188-191  fillSpec: fill_y_s, fill_z_s. */
 int flame_fillSpec(const FlameGrid *g, flame_stream_t stream, double *rhoi);
 
+/* reactionProperty (run.jl:84-94), the mechanism initReact builds (reactions.jl:506-575), for the
+ * grid's ns species and nreacs reactions.  Every array is device memory in Julia's column-major
+ * layout: reaction_type (nreacs: 1 Arrhenius, 2 three-body, 3 falloff-Troe), sgm (nreacs:
+ * reactant minus product stoichiometric sum), vf / vr (ns, nreacs: stoichiometric coefficients),
+ * Arr (3, nreacs: A in m, mol, s units, b, E/R in K), ef (ns, nreacs: third-body efficiencies),
+ * loP (3, nreacs: the low-pressure Arrhenius of falloff reactions), Troe (4, nreacs). */
+typedef struct FlameReactions {
+    int32_t nreacs;
+    int32_t pad;
+    double atm; /* Pa */
+    const int64_t *reaction_type, *sgm, *vf, *vr;
+    const double *Arr, *ef, *loP, *Troe;
+} FlameReactions;
+
+/* reactions.jl:187-232  eval_gpu(U, Q, ρi, dt, thermo, react, tag): explicit finite-rate
+ * chemistry on the interior cells hotter than T_criteria (a constant in run.jl:12): ρi += ẇ W
+ * dt, U[5] gains the formation-enthalpy release, ρi is clipped and rescaled to ρ, then T (GetT),
+ * p and e of Q are updated.  thermo needs the full NASA-7 set (a7 enters the Gibbs energy). */
+int flame_eval_gpu(const FlameGrid *g, flame_stream_t stream, double *U, double *Q,
+                   double *rhoi, double dt, const FlameThermo *thermo,
+                   const FlameReactions *react, const int64_t *tag, double T_criteria);
+
+/* reactions.jl:235-309  eval_gpu_stiff(…): the point-implicit form, (I − A dt) Δρ = ẇ W dt with
+ * the production-rate Jacobian A (vproductionRate_Jac, :383-462) solved by Gaussian elimination
+ * with partial pivoting (:465-504).  The reference reads the formation coefficient as
+ * coeffs_lo[n, 6] here but coeffs_lo[6, n] in eval_gpu; transposed = 1 reproduces the former
+ * (the linear element n + 35 of the 7 x ns matrix), 0 uses coeffs_lo[6, n] as eval_gpu does. */
+int flame_eval_gpu_stiff(const FlameGrid *g, flame_stream_t stream, double *U, double *Q,
+                         double *rhoi, double dt, const FlameThermo *thermo,
+                         const FlameReactions *react, const int64_t *tag, double T_criteria,
+                         int transposed);
+
 /* solver.jl:388-391  `any(isnan, U)` every 10 steps, as a count: writes to the device unsigned
  * *count how many of the nv ghosted FP64 fields' values are NaN or infinite (the reference
  * tests NaN only; an infinity is as fatal).  The caller reads it and stops the case, the

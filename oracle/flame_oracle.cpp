@@ -27,6 +27,7 @@
 #include <omp.h>
 #endif
 #include <cstring>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -855,6 +856,172 @@ double oracle_cfl_max(const FlameGrid *g, const double *Q, const FlameMetrics *m
                 best = jmax(best, tot);
             }
     return best;
+}
+
+// ------------------------------------------------------------ reactions.jl finite-rate chemistry
+static double ipow(double x, long k) {  // the stoichiometric integer powers
+    double r = 1.0;
+    const long m = k < 0 ? -k : k;
+    for (long i = 0; i < m; ++i) r *= x;
+    return k < 0 ? 1.0 / r : r;
+}
+
+// gibbs, thermo.jl:163-191
+static void gibbs(double *gi, double T, double lgT, double invT, const FlameThermo *th, int ns) {
+    const double mlogT = 1 - lgT;
+    const double T1 = 0.5 * T;
+    const double T2 = 1.0 / 6.0 * T * T;
+    const double T3 = T1 * T2;
+    const double T4 = 1.8 * T2 * T2;
+    for (int n = 0; n < ns; ++n) {
+        const double *c = T < th->coeffs_sep[n] ? th->coeffs_lo + 7 * n : th->coeffs_hi + 7 * n;
+        gi[n] = c[0] * mlogT - c[1] * T1 - c[2] * T2 - c[3] * T3 - c[4] * T4 + c[5] * invT - c[6];
+    }
+}
+
+// vproductionRate (reactions.jl:311-380); with A non-null also the Jacobian of
+// vproductionRate_Jac (:383-462), A column-major ns x ns
+void oracle_production_rate(double *wdot, const double *sc, double *A, double T,
+                            const FlameThermo *th, const FlameReactions *M, int ns) {
+    std::vector<double> gi(ns), kf(M->nreacs), Kc(M->nreacs);
+    const double lgT = std::log(T);
+    const double invT = 1.0 / T;
+    for (int n = 0; n < M->nreacs; ++n)
+        kf[n] = M->Arr[3 * n] * std::exp(M->Arr[3 * n + 1] * lgT - M->Arr[3 * n + 2] * invT);
+    gibbs(gi.data(), T, lgT, invT, th, ns);
+    const double RsT = th->Ru / M->atm * 1e6 * T;
+    for (int n = 0; n < M->nreacs; ++n) {
+        double dg = 0;
+        for (int m = 0; m < ns; ++m) dg += gi[m] * double(M->vf[m + ns * n] - M->vr[m + ns * n]);
+        Kc[n] = ipow(RsT, M->sgm[n]) * std::exp(dg);
+    }
+    for (int n = 0; n < M->nreacs; ++n) {
+        double qf = kf[n];
+        double qr = qf / Kc[n];
+        for (int m = 0; m < ns; ++m) {
+            const long vf = M->vf[m + ns * n], vr = M->vr[m + ns * n];
+            if (vf != 0) qf *= ipow(sc[m], vf);
+            if (vr != 0) qr *= ipow(sc[m], vr);
+        }
+        double mix = 0.0;
+        if (M->reaction_type[n] == 2) {
+            for (int m = 0; m < ns; ++m) mix += M->ef[m + ns * n] * sc[m];
+            qf *= mix;
+            qr *= mix;
+        } else if (M->reaction_type[n] == 3) {
+            for (int m = 0; m < ns; ++m) mix += M->ef[m + ns * n] * sc[m];
+            const double *lo = M->loP + 3 * n, *tr = M->Troe + 4 * n;
+            const double redP = mix / kf[n] * lo[0] * std::exp(lo[1] * lgT - lo[2] * invT);
+            const double logPred = std::log10(redP);
+            const double a = tr[0];
+            const double logFcent = std::log10((1 - a) * std::exp(-T / tr[1]) +
+                                               a * std::exp(-T / tr[2]) + std::exp(-tr[3] * invT));
+            const double troe_c = -0.4 - 0.67 * logFcent;
+            const double troe_n = 0.75 - 1.27 * logFcent;
+            const double troe = (troe_c + logPred) / (troe_n - 0.14 * (troe_c + logPred));
+            const double F = std::pow(10.0, logFcent / (1.0 + troe * troe));
+            const double k1 = (redP / (1.0 + redP)) * F;
+            qf *= k1;
+            qr *= k1;
+        }
+        for (int m = 0; m < ns; ++m) {
+            wdot[m] += (qf - qr) * double(M->vr[m + ns * n] - M->vf[m + ns * n]);
+            if (A) {
+                const double invsc = 1 / (sc[m] + kEps);
+                const double Awf = double(M->vf[m + ns * n]) * qf * invsc;
+                const double Awr = double(M->vr[m + ns * n]) * qr * invsc;
+                for (int l = 0; l < ns; ++l)
+                    A[l + ns * m] += (Awf - Awr) * double(M->vr[l + ns * n] - M->vf[l + ns * n]);
+            }
+        }
+    }
+}
+
+// solve, reactions.jl:465-504 (a column-major ns x ns; a and b are overwritten)
+void oracle_solve(double *x, double *a, double *b, int ns) {
+    auto A = [a, ns](int i, int j) -> double & { return a[i + ns * j]; };
+    for (int k = 0; k < ns - 1; ++k) {
+        double fmax = std::fabs(A(k, k));
+        int kk = k;
+        for (int i = k + 1; i < ns; ++i) {
+            const double absa = std::fabs(A(i, k));
+            if (absa > fmax) fmax = absa, kk = i;
+        }
+        for (int j = k; j < ns; ++j) std::swap(A(k, j), A(kk, j));
+        std::swap(b[k], b[kk]);
+        for (int i = k + 1; i < ns; ++i) {
+            const double f = -A(i, k) / A(k, k);
+            for (int j = 0; j < ns; ++j) A(i, j) += f * A(k, j);
+            b[i] += f * b[k];
+        }
+    }
+    x[ns - 1] = b[ns - 1] / A(ns - 1, ns - 1);
+    for (int i = ns - 2; i >= 0; --i) {
+        x[i] = b[i];
+        for (int j = i + 1; j < ns; ++j) x[i] -= A(i, j) * x[j];
+        x[i] /= A(i, i);
+    }
+}
+
+// eval_gpu (stiff 0, reactions.jl:187-232) and eval_gpu_stiff (stiff 1, :235-309)
+void oracle_eval_chem(const FlameGrid *g, int stiff, double *U, double *Q, double *rhoi, double dt,
+                      const FlameThermo *th, const FlameReactions *M, const int64_t *tag,
+                      double Tcrit, int transposed) {
+    Dims D(g);
+    const long np = D.np;
+    const int ns = D.ns;
+#pragma omp parallel for schedule(static)
+    for (long k = D.ng; k < D.nz + D.ng; ++k)
+        for (long j = D.ng; j < D.ny + D.ng; ++j)
+            for (long i = D.ng; i < D.nx + D.ng; ++i) {
+                const long p = D.P(i, j, k);
+                if (tagat(tag, p) != 0) continue;
+                double T = Q[p + 5 * np];
+                if (!(T > Tcrit)) continue;
+                double sc[FLAME_MAX_NS], wdot[FLAME_MAX_NS], r[FLAME_MAX_NS], dr[FLAME_MAX_NS];
+                for (int n = 0; n < ns; ++n) {
+                    r[n] = rhoi[p + n * np];
+                    sc[n] = r[n] / th->mw[n] * 1e-6;
+                    wdot[n] = 0.0;
+                }
+                double dei = 0;
+                if (stiff) {
+                    std::vector<double> A(ns * ns, 0.0), A1(ns * ns);
+                    double drho[FLAME_MAX_NS];
+                    oracle_production_rate(wdot, sc, A.data(), T, th, M, ns);
+                    for (int l = 0; l < ns; ++l)
+                        for (int n = 0; n < ns; ++n)
+                            A1[n + ns * l] = (n == l ? 1.0 : 0.0) -
+                                             A[n + ns * l] * th->mw[n] / th->mw[l] * dt;
+                    for (int n = 0; n < ns; ++n) drho[n] = wdot[n] * th->mw[n] * 1e6 * dt;
+                    oracle_solve(dr, A1.data(), drho, ns);
+                    for (int n = 0; n < ns; ++n) {
+                        const double a6 = transposed ? th->coeffs_lo[n + 35] : th->coeffs_lo[5 + 7 * n];
+                        dei += -a6 * dr[n] * th->Ru / th->mw[n];
+                        r[n] += dr[n];
+                    }
+                } else {
+                    oracle_production_rate(wdot, sc, nullptr, T, th, M, ns);
+                    for (int n = 0; n < ns; ++n) {
+                        const double d = wdot[n] * th->mw[n] * 1e6 * dt;
+                        dei += -th->coeffs_lo[5 + 7 * n] * d * th->Ru / th->mw[n];
+                        r[n] += d;
+                    }
+                }
+                U[p + 4 * np] += dei;
+                const double rho = jmax(Q[p], kEps);
+                double sum = 0.0;
+                for (int n = 0; n < ns; ++n) r[n] = jmax(r[n], 0.0), sum += r[n];
+                for (int n = 0; n < ns; ++n) r[n] *= rho / sum;
+                for (int n = 0; n < ns; ++n) rhoi[p + n * np] = r[n];
+                double ein = Q[p + 6 * np];
+                ein += dei;
+                T = jmax(GetT(ein, r, th, ns), kEps);
+                const double pr = jmax(Pmixture(T, r, th, ns), kEps);
+                Q[p + 4 * np] = pr;
+                Q[p + 5 * np] = T;
+                Q[p + 6 * np] = ein;
+            }
 }
 
 // One SSP-RK3 stage exactly as solver.jl:298-326 orders it (IBM off, periodic fill in place of

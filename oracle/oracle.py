@@ -61,6 +61,9 @@ SIGS = {
     "oracle_fill_z": [G, P, P, P, P, TH, C.POINTER(abi.FlameInflow)],
     "oracle_fill_z_s": [G, P],
     "oracle_mixture_properties": [D, D, P, TH, P, I, P, P, P],
+    "oracle_production_rate": [P, P, P, D, TH, C.POINTER(abi.FlameReactions), I],
+    "oracle_solve": [P, P, P, I],
+    "oracle_eval_chem": [G, I, P, P, P, D, TH, C.POINTER(abi.FlameReactions), P, D, I],
     "oracle_rk_stage_seq": [G, I, D, P, P, P, P, P, M, TH, TR],
     "oracle_h_specs": [P, D, TH, I],
     "oracle_up7": [P],
