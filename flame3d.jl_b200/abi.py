@@ -115,6 +115,7 @@ SIGNATURES = {
     "flame_fill_z_s": [G, S, P],
     "flame_fillGhost": [G, S, P, P, P, P, TH, C.POINTER(FlameInflow), I, I],
     "flame_fillSpec": [G, S, P],
+    "flame_fillIB": [G, S, P, P, P, P, P, P, P, P, P, TH, D],
     "flame_cfl_max": [G, S, P, M, P],
     "flame_check_finite": [G, S, P, I, P],
     "flame_eval_gpu": [G, S, P, P, P, D, TH, C.POINTER(FlameReactions), P, D],

@@ -535,6 +535,58 @@ __global__ void k_cfl_max(Dims D, const double *__restrict__ Q, FlameMetrics m,
     if ((threadIdx.x & 31) == 0 && bits) atomicMax(out, bits);
 }
 
+// fillIB, boundary.jl:193-279 (15-point stencils, 1-based Julia indices)
+__global__ void k_fill_ib(Dims D, double *Q, double *U, double *rhoi, const int64_t *ni,
+                          const int64_t *nj, const int64_t *nk, const double *cd,
+                          const double *cn, const int64_t *tag, FlameThermo th, double Tw) {
+    long long i = blockIdx.x * (long long)BX + threadIdx.x;
+    long long j = blockIdx.y * (long long)BY + threadIdx.y;
+    long long k = blockIdx.z * (long long)BZ + threadIdx.z;
+    if (i >= D.tx || j >= D.ty || k >= D.tz) return;
+    const long long p = D.P(i, j, k), np = D.np;
+    if (tag[p] != 3) return;
+    const int ns = D.ns;
+    constexpr int NPT = 15;
+    long long q[NPT];
+    for (int m = 0; m < NPT; ++m)
+        q[m] = D.P(ni[m + NPT * p] - 1, nj[m + NPT * p] - 1, nk[m + NPT * p] - 1);
+    const double *cnp = cn + 16 * p, *cdp = cd + 16 * p;
+    double Yg[FLAME_MAX_NS];
+    for (int n = 0; n < ns; ++n) {  // Y: zero gradient
+        double sum = 0.0;
+        for (int m = 0; m < NPT; ++m) sum += cnp[m + 1] * (rhoi[q[m] + n * np] / Q[q[m]]);
+        Yg[n] = -sum / cnp[0];
+    }
+    double sum = 0.0;  // p: zero gradient
+    for (int m = 0; m < NPT; ++m) sum += cnp[m + 1] * Q[q[m] + 4 * np];
+    const double pg = -sum / cnp[0];
+    double vel[3];  // u, v, w: Dirichlet
+    for (int c = 0; c < 3; ++c) {
+        sum = 0.0;
+        for (int m = 0; m < NPT; ++m) sum += cdp[m + 1] * Q[q[m] + (1 + c) * np];
+        vel[c] = -sum / cdp[0];
+    }
+    double yow = 0;  // ρmixture, thermo.jl:29-35
+    for (int n = 0; n < ns; ++n) yow += Yg[n] / th.mw[n];
+    const double rho = pg / (th.Ru * Tw * yow);
+    double r[FLAME_MAX_NS];
+    for (int n = 0; n < ns; ++n) r[n] = Yg[n] * rho, rhoi[p + n * np] = r[n];
+    const double ei = internal_energy<0>(th, ns, Tw, r);
+    const double ug = vel[0], vg = vel[1], wg = vel[2];
+    Q[p + 6 * np] = ei;
+    Q[p] = rho;
+    Q[p + np] = ug;
+    Q[p + 2 * np] = vg;
+    Q[p + 3 * np] = wg;
+    Q[p + 4 * np] = pg;
+    Q[p + 5 * np] = Tw;
+    U[p] = rho;
+    U[p + np] = rho * ug;
+    U[p + 2 * np] = rho * vg;
+    U[p + 3 * np] = rho * wg;
+    U[p + 4 * np] = ei + 0.5 * rho * (ug * ug + vg * vg + wg * wg);
+}
+
 // Non-finite values of an array (solver.jl:388-391 tests isnan over U).
 __global__ void k_count_nonfinite(long long n, const double *__restrict__ A, unsigned int *count) {
     unsigned int c = 0;
@@ -800,6 +852,19 @@ int flame_fillGhost(const FlameGrid *g, flame_stream_t s, double *Q, double *U, 
 int flame_fillSpec(const FlameGrid *g, flame_stream_t s, double *rhoi) {
     if (int e = flame_fill_y_s(g, s, rhoi)) return e;
     return flame_fill_z_s(g, s, rhoi);
+}
+
+int flame_fillIB(const FlameGrid *g, flame_stream_t s, double *Q, double *U, double *rhoi,
+                 const int64_t *neari, const int64_t *nearj, const int64_t *neark,
+                 const double *c_d, const double *c_n, const int64_t *tag, const FlameThermo *th,
+                 double T_wall) {
+    if (int e = flame_check_grid(g, "flame_fillIB")) return e;
+    if (!Q || !U || !rhoi || !neari || !nearj || !neark || !c_d || !c_n || !tag || !th)
+        return flame_fail(FLAME_EINVAL, "flame_fillIB: NULL argument");
+    const Dims D = make_dims(*g);
+    k_fill_ib<<<grid_for(D.tx, D.ty, D.tz), kBlock, 0, s>>>(D, Q, U, rhoi, neari, nearj, neark,
+                                                            c_d, c_n, tag, *th, T_wall);
+    return flame_check_launch("flame_fillIB");
 }
 
 int flame_check_finite(const FlameGrid *g, flame_stream_t s, const double *A, int nv,

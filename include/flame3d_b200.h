@@ -173,6 +173,18 @@ int flame_mixture(const FlameGrid *g, flame_stream_t stream, const double *Q, co
  * are case-specific inflow / zero-gradient; all benchmark cases are periodic). */
 int flame_fill_periodic(const FlameGrid *g, flame_stream_t stream, double *A, int nv);
 
+/* boundary.jl:193-279  fillIB(Q, U, ρi, neari, nearj, neark, c_d, c_n, tag, thermo): at every
+ * immersed-boundary ghost point (tag == 3) Y and p take the zero-gradient value -Σ c_n[m+1] f_m
+ * / c_n[1] and u, v, w the Dirichlet value with c_d over the 15 stencil points (neari / nearj /
+ * neark: (15, Tx, Ty, Tz) Int64, 1-based as in Julia; c_d, c_n: (16, Tx, Ty, Tz)); T is the wall
+ * temperature (300 K in the reference, here T_wall); ρ from ρmixture, then ρi, e, Q and U.  The
+ * stencil points are read while ghost points are written, so, as in the reference, a stencil
+ * must not contain another ghost point for the result to be defined. */
+int flame_fillIB(const FlameGrid *g, flame_stream_t stream, double *Q, double *U, double *rhoi,
+                 const int64_t *neari, const int64_t *nearj, const int64_t *neark,
+                 const double *c_d, const double *c_n, const int64_t *tag,
+                 const FlameThermo *thermo, double T_wall);
+
 /* The inflow state of the reference's fills.  fill_x / fill_z hard-code it (boundary.jl:17-25,
  * 96-104): P = 79.8 Pa, T = 270.65 K, u = 1000 m/s, v = w = 0, Y(2) = 0.233, Y(5) = 0.767
  * (1-based species), every other Y zero; here the caller passes it. */

@@ -820,6 +820,57 @@ void oracle_fill_z(const FlameGrid *g, double *Q, double *U, double *rhoi, doubl
             }
 }
 
+// boundary.jl:193-279 (fillIB; 15-point stencils with 1-based Julia indices)
+void oracle_fill_ib(const FlameGrid *g, double *Q, double *U, double *rhoi, const int64_t *ni,
+                    const int64_t *nj, const int64_t *nk, const double *cd, const double *cn,
+                    const int64_t *tag, const FlameThermo *th, double Tw) {
+    Dims D(g);
+    const long np = D.np;
+    const int ns = D.ns;
+    const int NPT = 15;
+    for (long p = 0; p < np; ++p) {
+        if (tag[p] != 3) continue;
+        long q[15];
+        for (int m = 0; m < NPT; ++m)
+            q[m] = D.P(ni[m + NPT * p] - 1, nj[m + NPT * p] - 1, nk[m + NPT * p] - 1);
+        const double *cnp = cn + 16 * p, *cdp = cd + 16 * p;
+        double Yg[FLAME_MAX_NS];
+        for (int n = 0; n < ns; ++n) {
+            double sum = 0.0;
+            for (int m = 0; m < NPT; ++m) sum += cnp[m + 1] * (rhoi[q[m] + n * np] / Q[q[m]]);
+            Yg[n] = -sum / cnp[0];
+        }
+        double sum = 0.0;
+        for (int m = 0; m < NPT; ++m) sum += cnp[m + 1] * Q[q[m] + 4 * np];
+        const double pg = -sum / cnp[0];
+        double vel[3];
+        for (int c = 0; c < 3; ++c) {
+            sum = 0.0;
+            for (int m = 0; m < NPT; ++m) sum += cdp[m + 1] * Q[q[m] + (1 + c) * np];
+            vel[c] = -sum / cdp[0];
+        }
+        double yow = 0;
+        for (int n = 0; n < ns; ++n) yow += Yg[n] / th->mw[n];
+        const double rho = pg / (th->Ru * Tw * yow);
+        double r[FLAME_MAX_NS];
+        for (int n = 0; n < ns; ++n) r[n] = Yg[n] * rho, rhoi[p + n * np] = r[n];
+        const double ei = InternalEnergy(Tw, r, th, ns);
+        const double ug = vel[0], vg = vel[1], wg = vel[2];
+        Q[p + 6 * np] = ei;
+        Q[p] = rho;
+        Q[p + np] = ug;
+        Q[p + 2 * np] = vg;
+        Q[p + 3 * np] = wg;
+        Q[p + 4 * np] = pg;
+        Q[p + 5 * np] = Tw;
+        U[p] = rho;
+        U[p + np] = rho * ug;
+        U[p + 2 * np] = rho * vg;
+        U[p + 3 * np] = rho * wg;
+        U[p + 4 * np] = ei + 0.5 * rho * (ug * ug + vg * vg + wg * wg);
+    }
+}
+
 // boundary.jl:160-176
 void oracle_fill_z_s(const FlameGrid *g, double *rhoi) {
     Dims D(g);

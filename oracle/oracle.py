@@ -60,6 +60,7 @@ SIGS = {
     "oracle_fill_y": [G, P, P, P],
     "oracle_fill_z": [G, P, P, P, P, TH, C.POINTER(abi.FlameInflow)],
     "oracle_fill_z_s": [G, P],
+    "oracle_fill_ib": [G, P, P, P, P, P, P, P, P, P, TH, D],
     "oracle_mixture_properties": [D, D, P, TH, P, I, P, P, P],
     "oracle_production_rate": [P, P, P, D, TH, C.POINTER(abi.FlameReactions), I],
     "oracle_solve": [P, P, P, I],

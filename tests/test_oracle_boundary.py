@@ -110,3 +110,56 @@ def test_cfl_max_matches_host_rule(f3d, oracle, maker):
     cfl = case.info.get("cfl", 0.5)
     assert cfl / rate == case.dt  # the same rule, the same operation order, bit for bit
     assert math.isfinite(rate) and rate > 0
+
+
+def _ib_setup(case, seed=3, nghost=12):
+    """Immersed-boundary arrays in the reference's layout: tag (Tx, Ty, Tz) with a few ghost
+    points (3), each with a 15-point stencil of fluid points (1-based Julia indices) and
+    averaging coefficients (Y and p zero gradient, velocity mirrored)."""
+    rng = np.random.default_rng(seed)
+    sh = case.Q.shape[1:]                       # (Tz, Ty, Tx)
+    tz, ty, tx = sh
+    np_ = tz * ty * tx
+    tag = np.zeros(sh, dtype=np.int64)
+    flat = rng.choice(np_, size=nghost, replace=False)
+    tag.ravel()[flat] = 3
+    fluid = np.flatnonzero(tag.ravel() == 0)
+    ni = np.ones((np_, 15), dtype=np.int64)     # Julia (15, Tx, Ty, Tz): point-major rows
+    nj, nk = ni.copy(), ni.copy()
+    cd = np.zeros((np_, 16))
+    cn = np.zeros((np_, 16))
+    for p in flat:
+        pts = rng.choice(fluid, size=15, replace=False)
+        x, y, z = pts % tx, (pts // tx) % ty, pts // (tx * ty)
+        ni[p], nj[p], nk[p] = x + 1, y + 1, z + 1
+        cn[p, 0], cn[p, 1:] = -1.0, 1.0 / 15
+        cd[p, 0], cd[p, 1:] = 1.0, 1.0 / 15
+    return tag, ni, nj, nk, cd, cn, flat
+
+
+def test_fill_ib_averages_and_mirrors(f3d, oracle):
+    case = f3d.random_curvilinear(n=10, ns=3, seed=41)
+    Q, r = case.Q.copy(), case.rhoi.copy()
+    U = np.ascontiguousarray(case.U())
+    tag, ni, nj, nk, cd, cn, flat = _ib_setup(case)
+    P = oracle.ptr
+    I64 = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    oracle.load().oracle_fill_ib(C.byref(case.grid()), P(Q), P(U), P(r), I64(ni), I64(nj),
+                                 I64(nk), P(cd), P(cn), I64(tag), C.byref(case.thermo.to_c()),
+                                 300.0)
+    th = case.thermo
+    Qf, rf = case.Q.reshape(7, -1), case.rhoi.reshape(case.ns, -1)
+    for p in flat:
+        pts = (ni[p] - 1) + case.Q.shape[3] * ((nj[p] - 1) + case.Q.shape[2] * (nk[p] - 1))
+        Y = (rf[:, pts] / Qf[0, pts]).mean(axis=1)
+        pg = Qf[4, pts].mean()
+        rho = pg / (th.Ru * 300.0 * np.sum(Y / th.mw))
+        q = Q.reshape(7, -1)[:, p]
+        np.testing.assert_allclose(q[[1, 2, 3]], -Qf[1:4, pts].mean(axis=1), rtol=1e-13)
+        assert q[4] == pytest.approx(pg, rel=1e-14) and q[5] == 300.0
+        assert q[0] == pytest.approx(rho, rel=1e-13)
+        np.testing.assert_allclose(r.reshape(case.ns, -1)[:, p], Y * rho, rtol=1e-13)
+        e = th.internal_energy(np.array([300.0]), (Y * rho)[:, None])[0]
+        assert q[6] == pytest.approx(e, rel=1e-13)
+    keep = tag.ravel() != 3
+    assert np.array_equal(Q.reshape(7, -1)[:, keep], Qf[:, keep])  # only ghost points change

@@ -73,3 +73,32 @@ def test_cfl_max_bit_identical(f3d, oracle, cuda_ok, maker):
                                        C.byref(oracle.metrics_struct(m)))
     assert out.item() == ref
     assert case.info["cfl"] / out.item() == case.dt
+
+
+def test_fill_ib_bit_identical(f3d, oracle, cuda_ok):
+    import importlib
+
+    import torch
+    tb = importlib.import_module("test_oracle_boundary")
+    case = f3d.random_curvilinear(n=12, ns=4, seed=42)
+    Q, r = case.Q.copy(), case.rhoi.copy()
+    U = np.ascontiguousarray(case.U())
+    tag, ni, nj, nk, cd, cn, _ = tb._ib_setup(case, seed=5, nghost=40)
+    cd[cd != 0] *= np.random.default_rng(6).uniform(0.5, 1.5, np.count_nonzero(cd))
+    cn[cn != 0] *= np.random.default_rng(7).uniform(0.5, 1.5, np.count_nonzero(cn))
+    d = {k: _dev(v) for k, v in dict(Q=Q, U=U, r=r, ni=ni, nj=nj, nk=nk, cd=cd, cn=cn,
+                                     tag=tag).items()}
+    lib = f3d.load_library()
+    th = case.thermo.to_c()
+    f3d.abi.check(lib, lib.flame_fillIB(C.byref(case.grid()),
+                                        C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                        *(d[k].data_ptr() for k in ("Q", "U", "r", "ni", "nj",
+                                                                    "nk", "cd", "cn", "tag")),
+                                        C.byref(th), 300.0))
+    torch.cuda.synchronize()
+    P = oracle.ptr
+    I64 = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    oracle.load().oracle_fill_ib(C.byref(case.grid()), P(Q), P(U), P(r), I64(ni), I64(nj),
+                                 I64(nk), P(cd), P(cn), I64(tag), C.byref(th), 300.0)
+    for k, h in (("Q", Q), ("U", U), ("r", r)):
+        assert np.array_equal(d[k].cpu().numpy(), h), k
