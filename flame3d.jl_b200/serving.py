@@ -608,3 +608,49 @@ def fifo(requests: list[SolveRequest], device="cuda", precision: int = 0,
     if keep_results:
         rep["results"] = results
     return rep
+
+
+# ------------------------------------------------------------------------------- replicas
+def route(requests: list[SolveRequest], n_replicas: int, cost=None) -> list[list[SolveRequest]]:
+    """Assigns each request, in arrival order, to the replica (GPU) with the least work assigned
+    so far (cost: cell-stages by default; ties to the lowest index).  Deterministic; every
+    request goes to exactly one replica and keeps its arrival order there."""
+    cost = cost or (lambda r: r.cell_stages)
+    loads = [0.0] * n_replicas
+    out: list[list[SolveRequest]] = [[] for _ in range(n_replicas)]
+    for r in sorted(requests, key=lambda r: r.arrival):
+        k = min(range(n_replicas), key=lambda i: (loads[i], i))
+        out[k].append(r)
+        loads[k] += cost(r)
+    return out
+
+
+class MultiServer:
+    """One Server per GPU, requests routed up front by `route`; replicas share nothing (no
+    data-path collective), each runs its own stream of arrivals in its own host thread."""
+
+    def __init__(self, devices, **server_kwargs):
+        self.servers = [Server(d, **server_kwargs) for d in devices]
+
+    def run(self, requests: list[SolveRequest]) -> dict:
+        parts = route(requests, len(self.servers))
+        reports: list = [None] * len(self.servers)
+
+        def work(i):
+            with torch.cuda.device(self.servers[i].device):
+                reports[i] = self.servers[i].run(parts[i]) if parts[i] else None
+
+        with ThreadPoolExecutor(max_workers=len(self.servers)) as pool:
+            for f in [pool.submit(work, i) for i in range(len(self.servers))]:
+                f.result()
+        done = [r for r in reports if r]
+        cs = sum(r["cell_stages"] for r in done)
+        first = min((p["arrival"] for r in done for p in r["per_request"]), default=0.0)
+        last = max((p["finished"] for r in done for p in r["per_request"]
+                    if not math.isnan(p["finished"])), default=first)
+        return {"replicas": len(self.servers), "requests": len(requests),
+                "completed": sum(r["completed"] for r in done), "cell_stages": cs,
+                "makespan_s": last - first,
+                "mcell_stage_per_s": cs / (last - first) / 1e6 if last > first else None,
+                "per_replica": [{k: v for k, v in r.items() if k != "per_request"} if r else None
+                                for r in reports]}

@@ -192,3 +192,31 @@ def test_fifo_baseline_matches_server_fp64(f3d, cuda_ok):
         Qf, rf = base["results"][r.rid]
         Qs, rs = srv.results[r.rid]
         assert np.array_equal(Qf, Qs) and np.array_equal(rf, rs)
+
+
+def test_route_balances_and_keeps_order(f3d):
+    S = _serving(f3d)
+    reqs = S.request_stream(200, seed=21)
+    parts = S.route(reqs, 4)
+    got = sorted(r.rid for p in parts for r in p)
+    assert got == [r.rid for r in reqs]                       # each request exactly once
+    for p in parts:
+        assert [r.arrival for r in p] == sorted(r.arrival for r in p)
+    loads = [sum(r.cell_stages for r in p) for p in parts]
+    assert max(loads) - min(loads) <= max(r.cell_stages for r in reqs)  # greedy bound
+    assert S.route(reqs, 4) == parts                          # deterministic
+    assert S.route(reqs, 1) == [sorted(reqs, key=lambda r: r.arrival)]
+
+
+@pytest.mark.gpu
+def test_multiserver_on_one_gpu_equals_server(f3d, cuda_ok):
+    S = _serving(f3d)
+    reqs = _small_stream(S, count=4, seed=14)
+    ms = S.MultiServer(["cuda:0"], precision=1, keep_results=True)
+    rep = ms.run(reqs)
+    assert rep["completed"] == 4 and rep["replicas"] == 1
+    alone = S.Server(precision=1, keep_results=True)
+    alone.run(reqs)
+    for r in reqs:
+        for a, b in zip(ms.servers[0].results[r.rid], alone.results[r.rid]):
+            assert np.array_equal(a, b)
