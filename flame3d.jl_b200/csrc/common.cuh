@@ -234,9 +234,10 @@ __device__ __forceinline__ T minmod(T a, T b) {  // schemes.jl:26-28
     return (a * b > 0) ? ((fabs(a) > fabs(b)) ? b : a) : T(0);
 }
 
-// WENO-Z weights and combination, schemes.jl:152-162: the smoothness indicators come in the
-// arithmetic type T, the weights are formed in FP64 (in FP32, q = τ/(1e-26 + β) overflows when
-// a one-sided split makes β exactly 0, and ∞·0 would poison the flux).
+// WENO-Z weights and combination, schemes.jl:152-162, for the 1:1 kernels: the smoothness
+// indicators come in the arithmetic type T and the weights are formed in FP64 in the reference's
+// four-division form (in plain FP32, q = τ/(1e-26 + β) overflows when a one-sided split makes β
+// exactly 0, and ∞·0 would poison the flux; wenoz_combine_fast<float> below avoids that).
 template <typename T>
 __device__ __forceinline__ T wenoz_combine(T s11_, T s22_, T s33_, T v1, T v2, T v3) {
     const double s11 = s11_, s22 = s22_, s33 = s33_;

@@ -19,8 +19,8 @@
 // Template parameters: a tile configuration, NS species (compile-time loops), QT the storage
 // type of the primitive and transport arrays, CT the arithmetic type of split, reconstruction
 // and viscous fluxes.  The plain path is <cfg, NS, double, double>; the mixed path is
-// <cfg, NS, float, float> with U, Un, rho_i, metrics, accumulators, the WENO-Z weights and the
-// Newton solve kept in FP64.
+// <cfg, NS, float, float> (reconstruction with its WENO-Z weights in FP32, wenoz_combine_fast
+// <float>) with U, Un, rho_i, metrics, accumulators and the Newton solve kept in FP64.
 //
 // All indices are 32-bit: the host checks that every array holds fewer than 2^31 elements.
 

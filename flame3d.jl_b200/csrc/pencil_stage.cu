@@ -16,6 +16,11 @@
 //   so its stores coalesce) finishes the stage: div (div.jl), RK3 combination (utils.jl:95-112),
 //   c2Prim with the Newton temperature (utils.jl:2-48, thermo.jl:231-282), the transport law of
 //   the new state, and the periodic ghost images.
+// Configurations (flame_rk_stage_tiled): 3 as above; 4 moves the finish into k_finish, one
+// thread per cell; 5 and 6 are 3 and 4 with each z / y sweep split into a flow sweep (the NS = 0
+// instance of the same kernel) and a species sweep (PART 2: species fluxes and the
+// enthalpy-diffusion term of the energy flux, with fewer slots and registers).  The flame_batch_*
+// persistent kernels at the end of the file run configuration 3 over many cases.
 //
 // Template parameters as in fused_stage.cu: NS species, QT storage of Q / transport, CT
 // arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
