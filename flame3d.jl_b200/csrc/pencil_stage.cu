@@ -60,7 +60,8 @@ struct Args {
     const double *met[10];
     const QT *metq;  // the metrics rounded to QT once (mixed precision), or null
     QT *aux;     // ϕ (1) and Y (NS), ghosted
-    double *R;   // right-hand side accumulator (5 + NS), ghosted indexing
+    double *R;   // right-hand side accumulator (5 + NS), ghosted indexing: z sweep, then all
+    double *R2;  // the y sweep's contribution (5 + NS), written, never read-modify-written
     FlameThermo th;
     FlameTransport tr;
 };
@@ -440,7 +441,7 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     for (int n = 0; n < 5; ++n) {
         const double u0 = A.U[g + n * np];
         if (A.stage == 1) A.Un[g + n * np] = u0;
-        double un = u0 + (A.R[g + n * np] + rhs[n]) * Jact;
+        double un = u0 + rhs[n] * Jact;
         if (A.stage > 1) un = un * A.ca + A.Un[g + n * np] * A.cb;
         Uc[n] = un;
         A.U[g + n * np] = un;
@@ -449,7 +450,7 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     for (int n = 0; n < NS; ++n) {
         const double r0 = A.ri[g + n * np];
         if (A.stage == 1) A.rn[g + n * np] = r0;
-        double rv = r0 + (A.R[g + (5 + n) * np] + rhs[5 + n]) * Jact;
+        double rv = r0 + rhs[5 + n] * Jact;
         if (A.stage > 1) rv = rv * A.ca + A.rn[g + n * np] * A.cb;
         r[n] = rv;
     }
@@ -530,7 +531,10 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
     const int g = gx + A.sy * gy + A.sz * gz;
     if (lane >= 3 && lane < 3 + OWN && a < A.nx) {  // what the end of this sweep reads
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
+        for (int n = 0; n < 5 + NS; ++n) {
+            prefetch_l2(A.R + g + n * A.np);
+            prefetch_l2(A.R2 + g + n * A.np);
+        }
         if constexpr (FIN) {
 #pragma unroll
             for (int n = 0; n < 5; ++n) {
@@ -556,15 +560,16 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
     }
     __syncwarp();
     if (lane < 3 || lane >= 3 + OWN || a >= A.nx) return;
-    double rhs[5 + NS];
+    double rhs[5 + NS];  // the complete right-hand side: (z + y) + x, one rounding per sum
 #pragma unroll
     for (int n = 0; n < 5 + NS; ++n)
-        rhs[n] = double(S[(SL::G + n) * 32 + lane]) - double(S[(SL::G + n) * 32 + lane + 1]);
+        rhs[n] = (A.R[g + n * A.np] + A.R2[g + n * A.np]) +
+                 (double(S[(SL::G + n) * 32 + lane]) - double(S[(SL::G + n) * 32 + lane + 1]));
     if constexpr (FIN) {
         finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
     } else {
 #pragma unroll
-        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * A.np] += rhs[n];
+        for (int n = 0; n < 5 + NS; ++n) A.R[g + n * A.np] = rhs[n];
     }
 }
 
@@ -575,17 +580,18 @@ __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_co
 }
 
 // The stage's finish for configuration 4: one thread per interior cell, x fastest, with the
-// complete right-hand side already in R.
+// complete right-hand side already in R (the x sweep summed it).
 template <int NS, typename QT>
 __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT> A) {
     const int c = blockIdx.x * 128 + threadIdx.x;
     if (c >= A.nx * A.ny * A.nz) return;
     const int x = c % A.nx, y = (c / A.nx) % A.ny, z = c / (A.nx * A.ny);
     const int gx = x + A.ng, gy = y + A.ng, gz = z + A.ng;
+    const int g = gx + A.sy * gy + A.sz * gz;
     double rhs[5 + NS];
 #pragma unroll
-    for (int n = 0; n < 5 + NS; ++n) rhs[n] = 0.0;
-    finish_cell<NS, QT>(A, gx + A.sy * gy + A.sz * gz, gx, gy, gz, rhs);
+    for (int n = 0; n < 5 + NS; ++n) rhs[n] = A.R[g + n * A.np];
+    finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
 }
 
 // Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
@@ -630,15 +636,13 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     const int seg = bid % nseg, c2 = bid / nseg;
     if (c2 >= n_c2) return;
     const int tid = threadIdx.x;
-    if constexpr (PASS == 1) {  // the R this thread adds to in phase C: start fetching it now
+    if constexpr (PASS == 1 && PART == 2) {  // the energy field this thread adds to in phase C
         const int cx = tid % COLS, l = tid / COLS;
         const int x = xb * COLS + cx, ac = seg * OWN - 3 + l;
         if (l >= 3 && l < 3 + OWN && ac < n_along && x < A.nx) {
             const int gy = DIR == 1 ? ac + A.ng : c2 + A.ng;
             const int gz = DIR == 1 ? c2 + A.ng : ac + A.ng;
-            const int g = (x + A.ng) + A.sy * gy + A.sz * gz;
-#pragma unroll
-            for (int n = (PART == 2 ? 4 : 0); n < 5 + NS; ++n) prefetch_l2(A.R + g + n * A.np);
+            prefetch_l2(A.R2 + (x + A.ng) + A.sy * gy + A.sz * gz + 4 * A.np);
         }
     }
     // ---- phase A, x-fastest: thread -> (column cx, pencil position l)
@@ -681,11 +685,13 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
 #pragma unroll
     for (int n = 0; n < NG_OUT; ++n) {
         const double d = double(Sc[(SL::G + n) * 32 + l]) - double(Sc[(SL::G + n) * 32 + l + 1]);
-        // PART 2: G[n] is species n (R field 5 + n) and G[NS] the energy term (R field 4,
-        // written by the flow sweep of this direction just before)
+        // the z sweep (PASS 0) writes R, the y sweep (PASS 1) R2; PART 2: G[n] is species n
+        // (field 5 + n) and G[NS] the energy term, added to field 4, which the flow sweep of
+        // the same direction wrote just before
+        double *Rt = PASS == 0 ? A.R : A.R2;
         const int f = PART == 2 ? (n < NS ? 5 + n : 4) : n;
-        if (PASS == 0 && !(PART == 2 && n == NS)) A.R[g + f * A.np] = d;
-        else A.R[g + f * A.np] += d;
+        if (PART == 2 && n == NS) Rt[g + f * A.np] += d;
+        else Rt[g + f * A.np] = d;
     }
 }
 
@@ -766,9 +772,10 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
                             m.detadz,  m.dzetadx, m.dzetady, m.dzetadz, m.J};
     for (int i = 0; i < 10; ++i) A.met[i] = mm[i];
     A.metq = sizeof(QT) == 4 ? static_cast<const QT *>(b.metrics_lo) : nullptr;
-    // scratch: R (5 + NS doubles per point) first, then ϕ and Y (1 + NS of QT per point)
+    // scratch: R and R2 (5 + NS doubles per point each) first, then ϕ and Y (1 + NS of QT)
     A.R = static_cast<double *>(scratch);
-    A.aux = reinterpret_cast<QT *>(A.R + (size_t)(5 + g.ns) * A.np);
+    A.R2 = A.R + (size_t)(5 + g.ns) * A.np;
+    A.aux = reinterpret_cast<QT *>(A.R2 + (size_t)(5 + g.ns) * A.np);
     A.th = th, A.tr = tr;
     return A;
 }
@@ -873,7 +880,7 @@ extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
     if (!g) return 0;
     const size_t np = (size_t)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
     const size_t q = precision == 0 ? sizeof(double) : sizeof(float);
-    return np * ((5 + g->ns) * sizeof(double) + (1 + g->ns) * q);
+    return np * (2 * (5 + g->ns) * sizeof(double) + (1 + g->ns) * q);
 }
 
 // ============================================================================= batches

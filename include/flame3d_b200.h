@@ -334,8 +334,8 @@ int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, d
                          const FlameThermo *thermo, const FlameTransport *transport,
                          int precision, int tile);
 
-/* Bytes of scratch the pencil configuration needs: (5 + ns) doubles and (1 + ns) values of the
- * storage type per ghosted point. */
+/* Bytes of scratch the pencil configurations need: 2 (5 + ns) doubles (the right-hand side of
+ * the z sweep and of the y sweep) and (1 + ns) values of the storage type per ghosted point. */
 size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision);
 
 /* No counterpart in the reference.  The pencil-sweep stage (configuration 3) for callers that
