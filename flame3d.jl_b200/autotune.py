@@ -3,7 +3,8 @@
 Configurations (flame_rk_stage_tiled): 0, 1, 2 = one tile kernel per stage (16x8x8 with one or
 two CTAs per SM, 8x8x8); 3 = prep + z, y, x pencil sweeps, the x sweep finishing the stage;
 4 = the same sweeps with the finish in its own per-cell launch; 5, 6 = 3, 4 with each y / z
-sweep split into a flow sweep and a species sweep.  Which is fastest depends on
+sweep split into a flow sweep and a species sweep.  The mixture-averaged transport (law 2) runs
+on the pencil configurations only (as 6); the tile configurations refuse it and are skipped.  Which is fastest depends on
 the species count (registers and shared memory per point grow with it), on the grid size (the
 tile kernels launch once per stage, which matters for small grids) and on the precision.
 
@@ -34,8 +35,10 @@ def size_class(cells: int) -> int:
     return int(round(math.log2(max(cells, 1))))
 
 
-def key(gpu: str, precision: int, ns: int, cells: int) -> str:
-    return f"{gpu}|p{precision}|ns{ns}|c{size_class(cells)}"
+def key(gpu: str, precision: int, ns: int, cells: int, law: int = 1) -> str:
+    """The cache key; the mixture-averaged transport (law 2) is tuned apart (its candidates and
+    its costs differ)."""
+    return f"{gpu}|p{precision}|ns{ns}|c{size_class(cells)}" + ("|law2" if law == 2 else "")
 
 
 class Autotuner:
@@ -77,7 +80,8 @@ class Autotuner:
 
     def choose(self, dc, gpu: str | None = None) -> int:
         gpu = gpu or self.gpu_name(dc.device)
-        k = key(gpu, dc.precision, dc.case.ns, dc.case.cells)
+        law = getattr(getattr(dc, "transport", None), "law", 1)
+        k = key(gpu, dc.precision, dc.case.ns, dc.case.cells, law)
         with self._lock:
             hit = self.table.get(k)
             if hit is not None:

@@ -495,6 +495,24 @@ __device__ __forceinline__ void mixture_properties(double T, double P, const dou
     }
 }
 
+// The reference's mixture kernel at one point with law 2 (thermo.jl:371-403): Y = max(ρi/ρ, 0)
+// with ρ = max(Q_ρ, eps), X from Y (Y2X, thermo.jl:38-52), then mixtureProperties.  The fused
+// stage stores the result as μ, λ, D_0 .. D_{NS-1}.
+template <int NS>
+__device__ __forceinline__ void mixture_point(const FlameThermo &th, const FlameTransport &tr,
+                                              double T, double P, double rho_raw, const double *r,
+                                              double &mu, double &lam, double *Dk) {
+    const double rhoinv = 1 / jmax(rho_raw, kEps);
+    double X[NS], mui[NS], W[NS * NS];
+    double yow = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) X[n] = jmax(r[n] * rhoinv, 0.0), yow += X[n] / th.mw[n];
+    const double yowinv = 1 / yow;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) X[n] = X[n] / th.mw[n] * yowinv;
+    mixture_properties(T, P, X, th, tr.poly, NS, W, mui, Dk, 1, lam, mu);
+}
+
 // An NVTX range over a host-side scope (stage launches show up by name in Nsight timelines).
 struct NvtxRange {
     explicit NvtxRange(const char *name) { nvtxRangePushA(name); }

@@ -557,6 +557,23 @@ __global__ void k_transport(int np, const QT *__restrict__ Q, const double *__re
     To[c] = QT(mu), To[c + np] = QT(lam), To[c + 2 * np] = QT(D);
 }
 
+// The same with the mixture-averaged law (law 2): μ, λ and the per-species D_k (fields 2 + n).
+template <int NS, typename QT>
+__global__ void k_transport_mix(int np, const QT *__restrict__ Q, const double *__restrict__ ri,
+                                QT *__restrict__ To, const FlameThermo th,
+                                const FlameTransport tr) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    double r[NS], Dk[NS], mu, lam;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) r[n] = ri[c + n * np];
+    mixture_point<NS>(th, tr, double(Q[c + 5 * np]), double(Q[c + 4 * np]), double(Q[c]), r, mu,
+                      lam, Dk);
+    To[c] = QT(mu), To[c + np] = QT(lam);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) To[c + (2 + n) * np] = QT(Dk[n]);
+}
+
 template <typename QT>
 Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuffers &b,
                    const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr) {
@@ -644,8 +661,11 @@ int transport_ns(int ns, int np, cudaStream_t s, const void *Q, const double *ri
     const QT *q = static_cast<const QT *>(Q);
     QT *t = static_cast<QT *>(To);
     switch (ns) {
-#define CASE(N) \
-    case N: k_transport<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr); break;
+#define CASE(N)                                                                  \
+    case N:                                                                      \
+        if (tr.law == 2) k_transport_mix<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr); \
+        else k_transport<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr);    \
+        break;
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
         default: return flame_fail(FLAME_EUNSUPPORTED, "flame_transport: ns=%d", ns);
@@ -674,12 +694,10 @@ extern "C" int flame_transport(const FlameGrid *g, flame_stream_t s, const void 
     if (int e = check_sizes(g, "flame_transport")) return e;
     if (!Q || !rhoi || !trans || !th || !tr)
         return flame_fail(FLAME_EINVAL, "flame_transport: NULL argument");
-    if (tr->law == 2)
-        return flame_fail(FLAME_EUNSUPPORTED,
-                          "flame_transport: law 2 (mixture-averaged, per-species D_k) runs on the "
-                          "per-kernel path (flame_mixture); the fused stage takes laws 0 and 1");
-    if (tr->law != 0 && tr->law != 1)
+    if (tr->law < 0 || tr->law > 2)
         return flame_fail(FLAME_EINVAL, "flame_transport: transport law %d unknown", tr->law);
+    if (tr->law == 2 && !tr->poly)
+        return flame_fail(FLAME_EINVAL, "flame_transport: law 2 needs the polynomial fits (poly)");
     const int np = (g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
     if (precision == 0)
         return flame::fused::transport_ns<double>(g->ns, np, s, Q, rhoi, trans, *th, *tr);
@@ -703,10 +721,14 @@ extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int st
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: NULL argument");
     if (stage < 1 || stage > 3)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: stage=%d must be 1, 2 or 3", stage);
-    if (tr->law != 0 && tr->law != 1)
-        return flame_fail(tr->law == 2 ? FLAME_EUNSUPPORTED : FLAME_EINVAL,
-                          "flame_rk_stage: transport law %d; the fused stage takes laws 0 and 1 "
-                          "(law 2 runs on the per-kernel path)", tr->law);
+    if (tr->law < 0 || tr->law > 2)
+        return flame_fail(FLAME_EINVAL, "flame_rk_stage: transport law %d unknown", tr->law);
+    if (tr->law == 2 && !tr->poly)
+        return flame_fail(FLAME_EINVAL, "flame_rk_stage: law 2 needs the polynomial fits (poly)");
+    if (tr->law == 2 && tile >= 0 && tile <= 2)
+        return flame_fail(FLAME_EUNSUPPORTED,
+                          "flame_rk_stage: transport law 2 (per-species D_k) runs on the pencil "
+                          "configurations 3-6, not on tile configuration %d", tile);
     if ((g->periodic & 7) != 7)
         return flame_fail(FLAME_EUNSUPPORTED,
                           "flame_rk_stage: the fused stage needs a grid periodic in x, y and z; "
@@ -716,8 +738,6 @@ extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int st
     if (b->Q_in == b->Q_out || (const void *)b->rhoi_in == (const void *)b->rhoi_out ||
         b->trans_in == b->trans_out)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: in and out buffers must differ");
-    if (tr->law != 0 && tr->law != 1)
-        return flame_fail(FLAME_EINVAL, "flame_rk_stage: transport law %d unknown", tr->law);
     if (precision == 0)
         return flame::fused::dispatch_tile<double, double>(tile, g->ns, *g, s, stage, dt, *b, *m,
                                                            *th, *tr);

@@ -283,8 +283,13 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 // The species part runs one species at a time in two passes (the sums of the diffusion
 // velocities first, then each species' reconstruction, corrected diffusion flux and enthalpy
 // flux), recomputing the few gradient terms instead of holding per-species arrays in registers.
-template <int DIR, int NS, typename QT, typename CT, int PART = 0>
-__device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G) {
+// MIXD (the mixture-averaged law, law 2): each species has its own D_k; Dk points at D_0 of
+// point l in the transport fields (field 2 + n holds D_n) and dstep is the pencil's stride, so
+// point l - 1 is Dk - dstep.  The other laws use the one D of the shared-memory slots and
+// compile without the per-species loads.
+template <int DIR, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
+__device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G,
+                                           const QT *Dk, int dstep) {
     using SL = SlotsOf<NS, PART>;
     constexpr int GS = PART == 2 ? 0 : 5;  // G index of species 0
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
@@ -312,8 +317,13 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
     const CT Tf = (SV(SL::T, lm) + SV(SL::T, l)) * h;
     const CT *md = met + 3 * DIR;
     // species diffusion (viscous.jl:430-507): the diffusion velocity of species n at the face
-    const CT rhoDi = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
+    const CT rhoD1 = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
     auto diffusion = [&](int n, CT &Vx, CT &Vy, CT &Vz) {
+        CT rhoDi = rhoD1;
+        if constexpr (MIXD) {
+            const QT *dn = Dk + (size_t)n * A.np;
+            rhoDi = (CT(dn[-dstep]) + CT(dn[0])) * rho;
+        }
         const CT y0 = SV(SL::Y + n, l), ym = SV(SL::Y + n, lm);
         const CT yp = SV(SL::Y + n, l + 1), ymm = SV(SL::Y + n, l - 2);
         CT dY[3];
@@ -431,7 +441,8 @@ __device__ __forceinline__ void species_point_phase(const Args<QT> &A, CT *S, in
 }
 
 // ---- last sweep: div, RK3 combination, c2Prim, transport, ghost images of one cell.
-template <int NS, typename QT>
+// LAW2: the mixture-averaged transport, written as μ, λ, D_0 .. D_{NS-1}.
+template <int NS, typename QT, bool LAW2 = false>
 __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, int gy, int gz,
                                             const double *rhs) {
     const int np = A.np;
@@ -466,23 +477,30 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     const double u = Uc[1] * rinv, v = Uc[2] * rinv, w = Uc[3] * rinv;
     const double ei = jmax(Uc[4] - 0.5 * rho * (u * u + v * v + w * w), kEps);
     double mu, lam, D, Tn, p;
+    double Dk[LAW2 ? NS : 1];
     if constexpr (NS < 4) {  // few species: the per-species sums are as cheap
         Tn = jmax(get_T<NS>(A.th, NS, ei, r), kEps);
         p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
-        transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
+        if constexpr (!LAW2) transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
     } else {  // the mixture's own polynomials (MixPoly): one evaluation per Newton iteration
         const MixPoly<NS> M(A.th, r);
         Tn = jmax(get_T_mix<NS>(M, A.th, ei, r), kEps);
         p = jmax(p_mixture<NS>(A.th, NS, Tn, r), kEps);
-        if (A.tr.law == 0) {
-            mu = A.tr.mu_ref, lam = A.tr.lambda_ref, D = A.tr.D_ref;
-        } else {  // transport_point with cp_mix = Σ_n w_n cp_n / ρ from the same polynomials
-            const double rh = jmax(rho, kEps);
-            const double cpm = (M.cv(Tn) + A.th.Ru * M.wsum) / rh;
-            mu = A.tr.mu_ref * pow(Tn / A.tr.T_ref, A.tr.exponent);
-            lam = cpm * mu / A.tr.Pr;
-            D = lam / (rh * cpm);
+        if constexpr (!LAW2) {
+            if (A.tr.law == 0) {
+                mu = A.tr.mu_ref, lam = A.tr.lambda_ref, D = A.tr.D_ref;
+            } else {  // transport_point with cp_mix = Σ_n w_n cp_n / ρ from the same polynomials
+                const double rh = jmax(rho, kEps);
+                const double cpm = (M.cv(Tn) + A.th.Ru * M.wsum) / rh;
+                mu = A.tr.mu_ref * pow(Tn / A.tr.T_ref, A.tr.exponent);
+                lam = cpm * mu / A.tr.Pr;
+                D = lam / (rh * cpm);
+            }
         }
+    }
+    if constexpr (LAW2) {  // the next stage's mixture kernel (thermo.jl:371-403), per cell
+        mixture_point<NS>(A.th, A.tr, Tn, p, rho, r, mu, lam, Dk);
+        D = Dk[0];
     }
     const double qv[7] = {rho, u, v, w, p, Tn, ei};
     const double tv[3] = {mu, lam, D};
@@ -506,6 +524,10 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
                 for (int n = 0; n < 7; ++n) A.Qo[t + n * np] = QT(qv[n]);
 #pragma unroll
                 for (int n = 0; n < 3; ++n) A.To[t + n * np] = QT(tv[n]);
+                if constexpr (LAW2) {
+#pragma unroll
+                    for (int n = 1; n < NS; ++n) A.To[t + (2 + n) * np] = QT(Dk[n]);
+                }
 #pragma unroll
                 for (int n = 0; n < NS; ++n) A.ro[t + n * np] = r[n];
             }
@@ -514,8 +536,9 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
 // x sweep (lanes along x, every access coalesced); it is the last sweep.  FIN: it finishes the
 // stage itself (configuration 3); otherwise it adds its differences to R and k_finish follows
 // (configuration 4: the FP64 finish then runs at full occupancy, apart from the sweep's
-// registers and shared memory).  Both round R + rhs once, so they agree bit for bit.
-template <int NS, typename QT, typename CT, bool FIN = true>
+// registers and shared memory).  Both form (R + R2) + rhs the same way, so they agree bit for
+// bit.
+template <int NS, typename QT, typename CT, bool FIN = true, bool MIXD = false>
 __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned char *smem_raw) {
     constexpr int WPB = Wpb<0>::value;
     using SL = Slots<NS>;
@@ -552,7 +575,7 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
     __syncwarp();
     CT G[5 + NS];
     const bool face = lane >= 3 && lane <= 3 + OWN && a <= A.nx;
-    if (face) face_phase<0, NS, QT, CT>(A, S, lane, G);
+    if (face) face_phase<0, NS, QT, CT, 0, MIXD>(A, S, lane, G, A.Ti + 2 * A.np + g, 1);
     __syncwarp();
     if (face) {
 #pragma unroll
@@ -573,15 +596,15 @@ __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned cha
     }
 }
 
-template <int NS, typename QT, typename CT, bool FIN>
+template <int NS, typename QT, typename CT, bool FIN, bool MIXD = false>
 __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    x_block<NS, QT, CT, FIN>(A, blockIdx.x, smem_raw);
+    x_block<NS, QT, CT, FIN, MIXD>(A, blockIdx.x, smem_raw);
 }
 
 // The stage's finish for configuration 4: one thread per interior cell, x fastest, with the
 // complete right-hand side already in R (the x sweep summed it).
-template <int NS, typename QT>
+template <int NS, typename QT, bool LAW2>
 __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT> A) {
     const int c = blockIdx.x * 128 + threadIdx.x;
     if (c >= A.nx * A.ny * A.nz) return;
@@ -591,7 +614,7 @@ __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT>
     double rhs[5 + NS];
 #pragma unroll
     for (int n = 0; n < 5 + NS; ++n) rhs[n] = A.R[g + n * A.np];
-    finish_cell<NS, QT>(A, g, gx, gy, gz, rhs);
+    finish_cell<NS, QT, LAW2>(A, g, gx, gy, gz, rhs);
 }
 
 // Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
@@ -620,7 +643,7 @@ struct Staged {
 // x-fastest threads (coalesced loads), then each warp works its own pencil from shared memory
 // exactly like the x sweep, and the right-hand side goes back with x-fastest threads.
 // PASS 0 writes R, PASS 1 adds to it.
-template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsigned char *smem_raw) {
     constexpr int COLS = Staged<NS, CT, PART>::COLS, STRIDE = Staged<NS, CT, PART>::STRIDE;
     using SL = SlotsOf<NS, PART>;
@@ -666,7 +689,14 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     const int a = seg * OWN - 3 + lane;
     CT G[NG_OUT];
     const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
-    if (face) face_phase<DIR, NS, QT, CT, PART>(A, S, lane, G);
+    if (face) {
+        // the lane's point in the transport fields (per-species D_k of law 2)
+        const int gxw = clampi(xb * COLS + warp, 0, A.nx - 1) + A.ng, gaw = a + A.ng;
+        const int gl = gxw + (DIR == 1 ? A.sy * gaw + A.sz * (c2 + A.ng)
+                                       : A.sy * (c2 + A.ng) + A.sz * gaw);
+        face_phase<DIR, NS, QT, CT, PART, MIXD>(A, S, lane, G, A.Ti + 2 * A.np + gl,
+                                          DIR == 1 ? A.sy : A.sz);
+    }
     __syncwarp();
     if (face) {
 #pragma unroll
@@ -695,11 +725,11 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     }
 }
 
-template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 __global__ void __launch_bounds__(Staged<NS, CT, PART>::COLS * 32)
     k_pencil_staged(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    staged_block<DIR, PASS, NS, QT, CT, PART>(A, blockIdx.x, smem_raw);
+    staged_block<DIR, PASS, NS, QT, CT, PART, MIXD>(A, blockIdx.x, smem_raw);
 }
 
 // ---------------------------------------------------------------------- batched, persistent
@@ -793,28 +823,28 @@ int set_smem(K kernel, size_t sm, bool *done) {
     return FLAME_OK;
 }
 
-template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0>
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 int launch_staged(const Args<QT> &A, cudaStream_t s) {
     using ST = Staged<NS, CT, PART>;
     constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
     static bool done[64] = {};
-    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART>, sm, done)) return e;
+    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD>, sm, done)) return e;
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
     const long long blocks = (long long)((A.nx + ST::COLS - 1) / ST::COLS) *
                              ((n_along + OWN - 1) / OWN) * n_c2;
-    k_pencil_staged<DIR, PASS, NS, QT, CT, PART><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
-template <int NS, typename QT, typename CT, bool FIN>
+template <int NS, typename QT, typename CT, bool FIN, bool MIXD = false>
 int launch_x(const Args<QT> &A, cudaStream_t s) {
     constexpr int WPB = Wpb<0>::value;
     constexpr size_t sm = smem_bytes<NS, CT, WPB>();
     static bool done[64] = {};
-    if (int e = set_smem(k_pencil_x<NS, QT, CT, FIN>, sm, done)) return e;
+    if (int e = set_smem(k_pencil_x<NS, QT, CT, FIN, MIXD>, sm, done)) return e;
     const long long warps = (long long)A.ny * A.nz * ((A.nx + OWN - 1) / OWN);
-    k_pencil_x<NS, QT, CT, FIN><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
+    k_pencil_x<NS, QT, CT, FIN, MIXD><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
@@ -825,6 +855,16 @@ int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const Flame
     const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr, scratch);
     k_prep<NS, QT><<<(unsigned)((A.np + 255) / 256), 256, 0, s>>>(A);
     if (int e = flame_check_launch("flame_rk_stage (prep)")) return e;
+    if (tr.law == 2) {  // per-species D_k: configuration 6's launches with the MIXD sweeps
+        if (int e = launch_staged<2, 0, 0, QT, CT>(A, s)) return e;
+        if (int e = launch_staged<2, 0, NS, QT, CT, 2, true>(A, s)) return e;
+        if (int e = launch_staged<1, 1, 0, QT, CT>(A, s)) return e;
+        if (int e = launch_staged<1, 1, NS, QT, CT, 2, true>(A, s)) return e;
+        if (int e = launch_x<NS, QT, CT, false, true>(A, s)) return e;
+        k_finish<NS, QT, true><<<(unsigned)(((long long)A.nx * A.ny * A.nz + 127) / 128), 128,
+                                  0, s>>>(A);
+        return flame_check_launch("flame_rk_stage (finish)");
+    }
     if (split_species) {  // configurations 5, 6: flow sweep (the NS = 0 instance) + species sweep
         if (int e = launch_staged<2, 0, 0, QT, CT>(A, s)) return e;
         if (int e = launch_staged<2, 0, NS, QT, CT, 2>(A, s)) return e;
@@ -837,7 +877,7 @@ int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const Flame
     if (!split_finish) return launch_x<NS, QT, CT, true>(A, s);
     if (int e = launch_x<NS, QT, CT, false>(A, s)) return e;
     const long long cells = (long long)A.nx * A.ny * A.nz;
-    k_finish<NS, QT><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(A);
+    k_finish<NS, QT, false><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(A);
     return flame_check_launch("flame_rk_stage (finish)");
 }
 
@@ -1051,7 +1091,10 @@ int check_case(const FlameCaseDesc &c, int i) {
         !b.trans_in || !b.trans_out || !b.scratch || !c.metrics.J || !c.metrics.dxidx)
         return flame_fail(FLAME_EINVAL, "flame_batch: case %d has a NULL buffer", i);
     if (c.transport.law != 0 && c.transport.law != 1)
-        return flame_fail(FLAME_EINVAL, "flame_batch: case %d transport law", i);
+        return flame_fail(c.transport.law == 2 ? FLAME_EUNSUPPORTED : FLAME_EINVAL,
+                          "flame_batch: case %d: transport law %d (the persistent batch takes "
+                          "laws 0 and 1; law 2 runs case by case on configurations 3-6)", i,
+                          c.transport.law);
     return FLAME_OK;
 }
 

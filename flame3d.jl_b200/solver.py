@@ -72,8 +72,10 @@ class DeviceCase:
         self.U = torch.empty((5,) + shp, **f64)
         self.Un = torch.empty((5,) + shp, **f64)
         self.rhon = torch.empty((ns,) + shp, **f64)
-        # μ, λ, D of the state, recomputed by every fused stage for the next one
-        self.T = [torch.empty((3,) + shp, dtype=qdt, device=dev) for _ in range(2)]
+        # μ, λ, D of the state, recomputed by every fused stage for the next one; with the
+        # mixture-averaged law (law 2) one D per species: μ, λ, D_0 .. D_{ns-1}
+        nt = 2 + ns if case.transport.law == 2 else 3
+        self.T = [torch.empty((nt,) + shp, dtype=qdt, device=dev) for _ in range(2)]
         if precision == 0:
             self._call("flame_prim2c", _p(self.U), _p(self.Q[0]))
         elif isinstance(case.Q, torch.Tensor):  # U from the FP64 primitives, before rounding
@@ -82,16 +84,14 @@ class DeviceCase:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
         self.scratch = None
         self.seq = None
-        if case.transport.law == 2:  # per-species D_k: the launch sequence only
-            self.tile = None
-        else:
-            self._transport()
-            # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice,
-            # or None for the pencil sweeps (configuration 3)
-            self.set_tile(3 if tile is None or tile == "auto" else tile)
-            if tile == "auto":
-                from . import autotune
-                self.set_tile(autotune.default().choose(self))
+        self._transport()
+        # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice, or
+        # None for the pencil sweeps (configuration 3; with law 2 the library runs the pencil
+        # configurations as 6)
+        self.set_tile(3 if tile is None or tile == "auto" else tile)
+        if tile == "auto":
+            from . import autotune
+            self.set_tile(autotune.default().choose(self))
         if sequence_buffers:
             self._alloc_sequence()
 
@@ -113,8 +113,7 @@ class DeviceCase:
         """After the primitive state was replaced (a restart): U from the FP64 primitives
         (prim2c, utils.jl:71-92) and the transport of the state for the fused stage."""
         self._call("flame_prim2c", _p(self.U), _p(q64.contiguous()))
-        if self.transport.law != 2:
-            self._transport()
+        self._transport()
 
     def set_tile(self, tile: int) -> None:
         """Switches the fused stage's configuration (the pencil ones need scratch)."""
@@ -223,20 +222,29 @@ class DeviceCase:
         abi.check(self.lib, rc)
         self.cur = o
 
+    @property
+    def launched_config(self) -> int:
+        """The configuration the library runs: the pencil configurations take the mixture-
+        averaged law (law 2) as configuration 6."""
+        if self.transport.law == 2 and self.tile in (3, 4, 5, 6):
+            return 6
+        return self.tile
+
     def launches_per_stage(self) -> int:
         """Kernels one fused stage launches: 4 for the pencil sweeps, one more with the
         separate finish (4, 6) and two more with split species sweeps (5, 6); 1 for a tile
         kernel."""
-        return {3: 4, 4: 5, 5: 6, 6: 7}.get(self.tile, 1)
+        return {3: 4, 4: 5, 5: 6, 6: 7}.get(self.launched_config, 1)
 
     def stage_kernels(self) -> str:
-        if self.tile in (3, 4, 5, 6):
-            yz = ("k_pencil_staged<z> + k_pencil_staged<y>" if self.tile < 5 else
+        t = self.launched_config
+        if t in (3, 4, 5, 6):
+            yz = ("k_pencil_staged<z> + k_pencil_staged<y>" if t < 5 else
                   "k_pencil_staged<z, flow> + k_pencil_staged<z, species> + "
                   "k_pencil_staged<y, flow> + k_pencil_staged<y, species>")
-            fin = " + k_finish" if self.tile in (4, 6) else ""
+            fin = " + k_finish" if t in (4, 6) else ""
             return f"pencil::k_prep + {yz} + k_pencil_x{fin}"
-        return "fused::k_stage<tile %d>" % self.tile
+        return "fused::k_stage<tile %d>" % t
 
     def step(self, fused: bool = True) -> None:
         torch.cuda.nvtx.range_push(f"step {self.case.name}")

@@ -75,7 +75,8 @@ typedef struct FlameThermo {
  *          caller in `poly`: visc_poly (5, ns), conduct_poly (5, ns), binarydiff_poly
  *          (5, ns, ns), each column-major as in thermoProperty, back to back (10 ns + 5 ns^2
  *          doubles, device memory for the GPU entry points).  Laws 0 and 1 run everywhere;
- *          law 2 runs on the per-kernel path (flame_mixture), whose D_k are per species. */
+ *          law 2 runs on the per-kernel path (flame_mixture) and on the fused stage's pencil
+ *          configurations 3-6, whose transport fields then hold one D_k per species. */
 typedef struct FlameTransport {
     int32_t law;
     int32_t pad;
@@ -292,7 +293,8 @@ int flame_specAdvance(const FlameGrid *g, flame_stream_t stream, double *rhoi, c
  * trans_out including their periodic ghost images, so the caller swaps every in/out pair after
  * each stage.  Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
  * trans_* hold the transport of the state, (…, 3) = μ, λ, D, as computed by flame_transport;
- * the stage computes the next one in its epilogue, so the law is evaluated once per cell.
+ * with law 2 (mixture-averaged, per-species D_k) they are (…, 2 + ns) = μ, λ, D_0 .. D_{ns-1}.
+ * The stage computes the next one in its epilogue, so the law is evaluated once per cell.
  * Q_* and trans_* are double arrays for precision 0 and float arrays for precision 1.
  * ------------------------------------------------------------------------------------- */
 typedef struct FlameStageBuffers {
@@ -303,8 +305,8 @@ typedef struct FlameStageBuffers {
     const double *rhoi_in; /* (…,ns) partial densities of the stage input, ghosts filled */
     double *rhoi_out;      /* (…,ns) partial densities of the stage result, ghosts filled */
     double *rhon;          /* (…,ns) RK3 stage-0 copy */
-    const void *trans_in;  /* (…,3) μ, λ, D of the stage input */
-    void *trans_out;       /* (…,3) μ, λ, D of the stage result */
+    const void *trans_in;  /* (…,3) μ, λ, D of the stage input; law 2: (…,2+ns) */
+    void *trans_out;       /* (…,3) μ, λ, D of the stage result; law 2: (…,2+ns) */
     void *scratch;         /* flame_stage_scratch_bytes() bytes for configurations 3 to 6,
                               else unused (may be NULL); contents need not survive calls */
     const void *metrics_lo; /* optional, precision 1 and configurations 3-4: the ten metric
@@ -328,7 +330,10 @@ int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double 
  * fifth, per-cell launch, bit-identical to 3; 5, 6 = configurations 3, 4 with each y / z sweep
  * split into a flow sweep and a species sweep (fewer registers and shared-memory slots per
  * sweep when there are many species).  The autotuner picks the configuration per grid,
- * species count and precision. */
+ * species count and precision.  Transport law 2 runs on configurations 3-6, always with
+ * configuration 6's launches (its species sweeps and x sweep read each species' D_k, and the
+ * finish evaluates the mixture rule per cell); configurations 0-2 refuse it with
+ * FLAME_EUNSUPPORTED. */
 int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                          const FlameStageBuffers *b, const FlameMetrics *m,
                          const FlameThermo *thermo, const FlameTransport *transport,
@@ -345,7 +350,7 @@ size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision);
  * lives in one array of FLAME_NOALLOC_SCRATCH_BYTES (64 MiB) that the library's GPU code holds
  * on every device it is loaded on until the process exits; b->scratch is ignored.  Grids whose
  * flame_stage_scratch_bytes() exceeds it are rejected with FLAME_EINVAL (FP64, ns = 1: up to
- * about one million ghosted points).  The first call on a device looks up the array's address
+ * about 600 thousand ghosted points).  The first call on a device looks up the array's address
  * with that device current, so make it before any stream capture.  All calls on a device share
  * the array: calls that overlap on the GPU race and must be serialised by the caller.  Nothing
  * in the array has to start at zero; allocates nothing. */
@@ -355,8 +360,9 @@ int flame_rk_stage_noalloc(const FlameGrid *g, flame_stream_t stream, int stage,
                            const FlameThermo *thermo, const FlameTransport *transport,
                            int precision);
 
-/* μ, λ, D of every ghosted point of a state (Q, rhoi) into trans (…, 3): the transport law of
- * flame_mixture without the mass-fraction output; starts the fused stage loop. */
+/* μ, λ, D of every ghosted point of a state (Q, rhoi) into trans (…, 3), or (…, 2 + ns) with
+ * law 2: the transport law of flame_mixture without the mass-fraction output; starts the fused
+ * stage loop. */
 int flame_transport(const FlameGrid *g, flame_stream_t stream, const void *Q, const double *rhoi,
                     void *trans, const FlameThermo *thermo, const FlameTransport *transport,
                     int precision);

@@ -1,7 +1,8 @@
-"""GPU parity of the mixture-averaged transport (law 2, thermo.jl:289-403) on the per-kernel
-path: flame_mixture against the oracle, and the reference launch sequence over two stages.
-log() and sqrt() come from different math libraries on the two sides, so the bound is a
-relative 1e-13 rather than bit equality."""
+"""GPU parity of the mixture-averaged transport (law 2, thermo.jl:289-403): flame_mixture
+against the oracle, the reference launch sequence over two stages, and the fused stage's pencil
+configurations (per-species D_k in the sweeps, the mixture rule in the finish) over two steps.
+log() and sqrt() come from different math libraries on the two sides, so the bound on the
+transport fields is a relative 1e-13 rather than bit equality, and 1e-12 on the stages."""
 from __future__ import annotations
 
 import ctypes as C
@@ -67,14 +68,85 @@ def test_launch_sequence_law2_matches_oracle(f3d, oracle, cuda_ok):
     assert np.linalg.norm((I(r) - I(oc.rhoi)).ravel()) <= 1e-12 * np.linalg.norm(I(oc.rhoi).ravel())
 
 
-def test_fused_stage_refuses_law2(f3d, cuda_ok):
+def test_tile_configs_refuse_law2(f3d, cuda_ok):
+    """The tile kernels hold one D per point; law 2 is refused there with FLAME_EUNSUPPORTED
+    (before any launch) and runs on the pencil configurations as configuration 6."""
     S = f3d.solver_module()
     case = _case(f3d, ns=3, seed=43)
     dc = S.DeviceCase(case)
-    assert dc.tile is None
+    assert dc.tile == 3 and dc.launched_config == 6 and dc.T[0].shape[0] == 2 + 3
     lib = f3d.load_library()
     b = f3d.FlameStageBuffers(*([1] * 10))
-    rc = lib.flame_rk_stage_tiled(C.byref(dc.grid), None, 1, 1e-6, C.byref(b),
-                                  C.byref(dc.cmetrics), C.byref(dc.thermo),
-                                  C.byref(dc.transport), 0, 3)
-    assert rc == 5 and "law 2" in f3d.abi.last_error(lib)
+    for tile in (0, 1, 2):
+        rc = lib.flame_rk_stage_tiled(C.byref(dc.grid), None, 1, 1e-6, C.byref(b),
+                                      C.byref(dc.cmetrics), C.byref(dc.thermo),
+                                      C.byref(dc.transport), 0, tile)
+        assert rc == 5 and "law 2" in f3d.abi.last_error(lib)
+
+
+def _stage_errors(dc, oc, oracle):
+    I = oracle.interior
+    U = dc.conserved()
+    mom = np.linalg.norm(I(oc.U[1:4]).ravel())
+    e = {}
+    for n in range(5):
+        ref = I(oc.U[n])
+        scale = mom if 1 <= n <= 3 else np.linalg.norm(ref.ravel())
+        e[f"U{n}"] = float(np.linalg.norm((I(U[n]) - ref).ravel()) / scale)
+    _, r = dc.primitives()
+    e["rhoi"] = oracle.rel_l2(I(r), I(oc.rhoi))
+    return e
+
+
+@pytest.mark.parametrize("tile", [3, 4, 6])
+@pytest.mark.parametrize("ns", [2, 5, 9])
+def test_fused_law2_matches_oracle(f3d, oracle, cuda_ok, ns, tile):
+    """Two RK3 steps of the fused stage with mixture-averaged transport against the oracle's
+    launch sequence (mixture kernel first in every stage): 1e-12 relative L2."""
+    S = f3d.solver_module()
+    case = _case(f3d, ns=ns, seed=50 + ns)
+    dc = S.DeviceCase(case, tile=tile)
+    oc = oracle.OracleCase(case)
+    for _ in range(2):
+        dc.step()
+        oc.step()
+    e = _stage_errors(dc, oc, oracle)
+    assert max(e.values()) <= 1e-12, e
+    assert np.isfinite(dc.conserved()).all()
+
+
+def test_fused_law2_transport_fields(f3d, oracle, cuda_ok):
+    """The transport fields the stage leaves for the next one: μ, λ and one D_k per species,
+    equal to the oracle's mixture kernel on the stage's own output state."""
+    import torch
+    S = f3d.solver_module()
+    case = _case(f3d, ns=5, seed=57)
+    dc = S.DeviceCase(case, tile=4)
+    dc.stage_fused(1)
+    torch.cuda.synchronize()
+    Q, r = dc.primitives()
+    T = dc.T[dc.cur].cpu().numpy()
+    shp, ns = Q.shape[1:], case.ns
+    ref = {k: np.zeros((n,) + shp) for k, n in (("Yi", ns), ("lam", 1), ("mu", 1), ("D", ns))}
+    P = oracle.ptr
+    Qc, rc = np.ascontiguousarray(Q), np.ascontiguousarray(r)
+    oracle.load().oracle_mixture(C.byref(case.grid()), P(Qc), P(rc), P(ref["Yi"]),
+                                 P(ref["lam"]), P(ref["mu"]), P(ref["D"]),
+                                 C.byref(case.thermo.to_c()), C.byref(case.transport.to_c()), None)
+    np.testing.assert_allclose(T[0], ref["mu"][0], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(T[1], ref["lam"][0], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(T[2:], ref["D"], rtol=1e-13, atol=0)
+
+
+def test_fused_law2_mixed_precision(f3d, oracle, cuda_ok):
+    """Mixed precision with law 2 (D_k stored in FP32): within the mixed path's 1e-5 bound of
+    the oracle after two steps."""
+    S = f3d.solver_module()
+    case = _case(f3d, ns=5, seed=58)
+    dc = S.DeviceCase(case, precision=1, tile=6)
+    oc = oracle.OracleCase(case)
+    for _ in range(2):
+        dc.step()
+        oc.step()
+    e = _stage_errors(dc, oc, oracle)
+    assert max(e["U0"], e["U4"], e["U1"]) <= 1e-5, e
