@@ -66,6 +66,8 @@ WORKLOADS = {
     "jet128x64x64": dict(kind="jet", nx=128, ny=64, nz=64),
     "tgv64": dict(kind="tgv", n=64),
     "mix192_ns9": dict(kind="mixing", n=192, ns=9),
+    # the reference's own transport: mixture-averaged (thermo.jl:289-369) with seeded fits
+    "mix96_ns9_law2": dict(kind="mixing", n=96, ns=9, law2=True),
     "ensemble64": dict(kind="ensemble"),
     "serve": dict(kind="serve"),
     "precision": dict(kind="precision"),
@@ -81,7 +83,11 @@ def make_case(f3d, name: str, nz_override: int | None = None):
         return f3d.curvilinear_jet(**w)
     if kind == "tgv":
         return f3d.taylor_green(**w)
-    return f3d.mixing_layer(**w)
+    law2 = w.pop("law2", False)
+    case = f3d.mixing_layer(**w)
+    if law2:
+        case.transport = f3d.cases.mixture_averaged_transport(case.thermo, seed=3)
+    return case
 
 
 # ------------------------------------------------------------------------------ clocks
