@@ -35,6 +35,7 @@ ROOT = Path(__file__).resolve().parent
 METRIC = "Mcell-stage/s plain FP64 vs batched mixed-prec; p50/p99 step latency at err"
 UNIT = "Mcell-stage/s"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
+E2E_LANES = 3  # cases / streams the end-to-end calls rotate over
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
 
 
@@ -536,14 +537,16 @@ def main() -> int:
     # ---- end to end through the host-buffer API (pinned host memory, copies timed).  Each
     # step is one call: upload Q, rho_i from pinned host memory, prim2c, one RK3 step, download
     # Q, rho_i.  Serial: one call after the other on one stream.  Pipelined (reported as e2e):
-    # independent calls alternate between two cases on two streams, so one call's copies run
-    # while the other computes (PCIe is full duplex); every step still makes its own copies.
+    # independent calls rotate over three cases on three streams, so while one call computes the
+    # others upload and download (PCIe is full duplex; a call's two copies together take about
+    # as long as its step, so two lanes leave the GPU idle between steps); every step still
+    # makes its own copies.
     ns = case.ns
     Qh = torch.from_numpy(case.Q).pin_memory()
     rh = torch.from_numpy(case.rhoi).pin_memory()
-    Qo = [torch.empty_like(Qh).pin_memory() for _ in range(2)]
-    ro = [torch.empty_like(rh).pin_memory() for _ in range(2)]
-    e2e_steps = max(4, min(args.steps, 20))
+    Qo = [torch.empty_like(Qh).pin_memory() for _ in range(E2E_LANES)]
+    ro = [torch.empty_like(rh).pin_memory() for _ in range(E2E_LANES)]
+    e2e_steps = E2E_LANES * max(2, min(args.steps, 21) // E2E_LANES)
     for _ in range(2):
         dc.advance_from_host(Qh, rh, 1, Qo[0], ro[0])
     barrier()
@@ -553,15 +556,15 @@ def main() -> int:
     e1.record(stream)
     barrier()
     ms_serial = max_over_ranks(e0.elapsed_time(e1), dev)
-    dcs = [dc, dc.clone()]
-    lanes = [torch.cuda.Stream(dev) for _ in range(2)]
-    for k in range(2):  # warm the second case and both streams
+    dcs = [dc] + [dc.clone() for _ in range(E2E_LANES - 1)]
+    lanes = [torch.cuda.Stream(dev) for _ in range(E2E_LANES)]
+    for k in range(E2E_LANES):  # warm the other cases and every stream
         with torch.cuda.stream(lanes[k]):
             dcs[k].advance_from_host(Qh, rh, 1, Qo[k], ro[k])
     barrier()
     e0.record(stream)
     for i in range(e2e_steps):
-        k = i % 2
+        k = i % E2E_LANES
         lanes[k].wait_event(e0)
         with torch.cuda.stream(lanes[k]):
             dcs[k].advance_from_host(Qh, rh, 1, Qo[k], ro[k])
@@ -588,7 +591,7 @@ def main() -> int:
     achieved = balg * cells / (stage_ms / 1e3) / 1e9
     traffic = None
     if TRAFFIC.exists():
-        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}:{dc.tile}")
+        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}:{dc.launched_config}")
         if tr:
             traffic = tr.get("bytes_per_stage")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -610,7 +613,7 @@ def main() -> int:
            "dtype": "f64" if prec == 0 else "f32/f64",
            "data": "synthetic (seeded jet on the wavy periodic mapping)",
            "config": {"workload": args.workload, "cells": cells, "species": ns,
-                      "precision": args.precision, "path": dc.stage_kernels(), "stage_config": dc.tile,
+                      "precision": args.precision, "path": dc.stage_kernels(), "stage_config": dc.launched_config,
                       "l2": "inputs larger than L2 (state ~%.1f GB per replica)" % (
                           (35 + 3 * ns) * case.Q[0].size * 8 / 1e9),
                       "parallelism": f"replicas x{world}"},
@@ -618,7 +621,7 @@ def main() -> int:
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                    "calls": "DeviceCase.advance_from_host, one RK3 step per call, independent "
-                            "calls alternating over 2 cases on 2 streams",
+                            f"calls rotating over {E2E_LANES} cases on {E2E_LANES} streams",
                    "serial_one_stream": e2e_serial},
            "gpu_launches": stages * dc.launches_per_stage()}
     print(json.dumps(out), flush=True)
