@@ -125,3 +125,28 @@ def test_graph_batch_with_mixed_configurations(f3d, cuda_ok):
         for a, c in zip(_state(x), _state(y)):
             assert np.array_equal(a, c)
     b.close()
+
+
+def test_graph_batch_with_law2_case(f3d, cuda_ok):
+    """A case with mixture-averaged transport (law 2, run as configuration 6) batched in graph
+    mode with law-1 cases ends bit for bit where it ends alone; the persistent batch, whose
+    kernels carry one D per point, refuses it with FLAME_EUNSUPPORTED."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)[:3]
+    law2 = f3d.random_curvilinear(n=12, ns=4, seed=55)
+    law2.transport = f3d.cases.mixture_averaged_transport(law2.thermo, seed=55)
+    cases.append(law2)
+    batched = [S.DeviceCase(c, tile=3) for c in cases]
+    alone = S.DeviceCase(law2, tile=3)
+    b = B.Batch(batched, mode="graph")
+    b.capture()
+    for _ in range(2):
+        b.step()
+        alone.step()
+    for a, c in zip(_state(alone), _state(batched[-1])):
+        assert np.array_equal(a, c)
+    b.close()
+    with pytest.raises(f3d.abi.FlameError) as e:
+        B.Batch([S.DeviceCase(law2, tile=3)], mode="persistent")
+    assert e.value.code == 5

@@ -150,3 +150,18 @@ def test_fused_law2_mixed_precision(f3d, oracle, cuda_ok):
         oc.step()
     e = _stage_errors(dc, oc, oracle)
     assert max(e["U0"], e["U4"], e["U1"]) <= 1e-5, e
+
+
+def test_fused_law2_odd_extents(f3d, oracle, cuda_ok):
+    """Odd, unequal extents (15 x 11 x 9): the per-species D_k loads of the sweeps follow the
+    pencils' strides, and the finish writes every ghost image."""
+    S = f3d.solver_module()
+    case = f3d.random_curvilinear(n=11, ns=3, seed=59)
+    case.transport = f3d.cases.mixture_averaged_transport(case.thermo, seed=59)
+    dc = S.DeviceCase(case, tile=6)
+    oc = oracle.OracleCase(case)
+    for _ in range(2):
+        dc.step()
+        oc.step()
+    e = _stage_errors(dc, oc, oracle)
+    assert max(e.values()) <= 1e-12, e
