@@ -623,14 +623,20 @@ __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT>
     finish_cell<NS, QT, LAW2>(A, g, gx, gy, gz, rhs, pw);
 }
 
-// Columns per block of the staged y / z sweeps: 16 consecutive x columns, so the block's loads
-// use whole 128-byte lines; 8 when the column slots would not fit in shared memory.  (Sizing
-// for two blocks per SM instead, 16/8/4 columns under 112 KB, measured 0-2 % faster with few
-// species and 6 % slower with nine.)  Host and device use this rule: the batch planner sizes
-// its work list with it.
+// Columns per block of the staged y / z sweeps.  Single precision: 16 consecutive x columns, so
+// the block's loads use whole 128-byte lines; 8 when the column slots would not fit in shared
+// memory.  (Sizing for two blocks per SM instead, 16/8/4 columns under 112 KB, measured 0-2 %
+// faster with few species and 6 % slower with nine.)  FP64 sweeps that carry species: always 8
+// columns.  With one or two species a 16-column FP64 block holds 172-199 KB, one block per SM,
+// and its warps wait at the phase barriers with nothing else to run; two 8-column blocks keep
+// the same warp count and one block's loads overlap the other's arithmetic (2-3 % faster on the
+// 256x128x128 jet, neutral with two species); from three species on 16 columns would not fit
+// anyway.  The flow-only sweep of configurations 5 and 6 (ns = 0) keeps 16 columns: 8 measured
+// 8 % slower there.  Host and device use this rule: the batch planner sizes its work list with
+// it.
 constexpr int slots_of(int ns) { return 37 + 5 * ns; }
 constexpr int staged_cols(int ns, size_t csz) {
-    return csz * slots_of(ns) * 33 * 16 <= 200 * 1024 ? 16 : 8;
+    return (csz == 8 && ns > 0) ? 8 : (csz * slots_of(ns) * 33 * 16 <= 200 * 1024 ? 16 : 8);
 }
 
 template <int NS, typename CT, int PART = 0>
