@@ -502,45 +502,63 @@ __device__ __forceinline__ void mixture_properties(double T, double P, const dou
 // the reference's loops (row n's terms l < n arrive in iteration n, its terms l > n in the
 // later iterations, in increasing order), and each term is the reference's expression.
 //
-// pw holds the terms of the Wilke factors that depend on the molar masses alone, filled once per
-// block by wilke_pairs_fill: for the pair (n, l) at n * NS + l, 1 / wr with wr = W_l / W_n,
-// sqrt(wr) and 1 / sqrt(8 + 8 / wr).  The per-point divisions of the reference's expressions
-// become products with reciprocals (1 / μ_l once per species, 1 / D_nm once per pair): the
-// same formulas, each term within a few ulps of the reference's, at a third of the FP64
-// divisions and square roots.
-template <int NS>
-__device__ __forceinline__ void wilke_pairs_fill(const FlameThermo &th, double *pw) {
+// The block's MixTables hold the terms of the Wilke factors that depend on the molar masses
+// alone (for the pair (n, l) at n * NS + l: 1 / wr with wr = W_l / W_n, sqrt(wr) and
+// 1 / sqrt(8 + 8 / wr), each formed in FP64).  The per-point divisions of the reference's
+// expressions become products with reciprocals (1 / μ_l once per species, 1 / D_nm once per
+// pair): the same formulas, each term within a few ulps of the reference's, at a third of the
+// divisions and square roots.  MT is the arithmetic type: double on the FP64 path; float on the
+// mixed path, which stores μ, λ and D_k in FP32 anyway (the tables then also hold the
+// polynomial fits rounded to FP32 once per block).
+template <int NS, typename MT>
+struct MixTables {
+    MT pw[3 * NS * NS];
+    MT poly[sizeof(MT) == 4 ? 10 * NS + 5 * NS * NS : 1];
+};
+
+template <int NS, typename MT>
+__device__ __forceinline__ void mix_tables_fill(const FlameThermo &th, const FlameTransport &tr,
+                                                MixTables<NS, MT> &t) {
     for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) {
         const int n = i / NS, l = i % NS;
         const double tmp1 = 1 / th.mw[n];
         const double wr = th.mw[l] * tmp1;
-        pw[i] = 1 / wr;
-        pw[NS * NS + i] = sqrt(wr);
-        pw[2 * NS * NS + i] = 1 / sqrt(8 + 8 / wr);
+        t.pw[i] = MT(1 / wr);
+        t.pw[NS * NS + i] = MT(sqrt(wr));
+        t.pw[2 * NS * NS + i] = MT(1 / sqrt(8 + 8 / wr));
+    }
+    if constexpr (sizeof(MT) == 4) {
+        for (int i = threadIdx.x; i < 10 * NS + 5 * NS * NS; i += blockDim.x)
+            t.poly[i] = MT(tr.poly[i]);
     }
 }
 
-template <int NS>
-__device__ __forceinline__ void mixture_properties_pairs(double T, double P, const double *X,
-                                                         const double *pw, const double *poly,
-                                                         double *Dk, double &lam, double &mu) {
-    const double *visc = poly, *cond = poly + 5 * NS, *bin = poly + 10 * NS;
-    const double sqT = sqrt(T), sqsqT = sqrt(sqT), lgT = log(T);
-    const double lgT2 = lgT * lgT, lgT3 = lgT * lgT2, lgT4 = lgT2 * lgT2;
-    double mui[NS], row[NS];
+template <typename MT>
+__device__ __forceinline__ MT dot5t(MT l1, MT l2, MT l3, MT l4, const MT *p) {
+    return p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3] + l4 * p[4];
+}
+
+template <int NS, typename MT>
+__device__ __forceinline__ void mixture_properties_pairs(MT T, MT P, const MT *X, const MT *pw,
+                                                         const MT *poly, MT *Dk, MT &lam,
+                                                         MT &mu) {
+    const MT *visc = poly, *cond = poly + 5 * NS, *bin = poly + 10 * NS;
+    const MT sqT = sqrt(T), sqsqT = sqrt(sqT), lgT = log(T);
+    const MT lgT2 = lgT * lgT, lgT3 = lgT * lgT2, lgT4 = lgT2 * lgT2;
+    MT mui[NS], row[NS];
 #pragma unroll
-    for (int n = 0; n < NS; ++n) mui[n] = sqT * dot5(lgT, lgT2, lgT3, lgT4, cond + 5 * n);
-    double sum1 = 0, sum2 = 0;
+    for (int n = 0; n < NS; ++n) mui[n] = sqT * dot5t<MT>(lgT, lgT2, lgT3, lgT4, cond + 5 * n);
+    MT sum1 = 0, sum2 = 0;
 #pragma unroll
     for (int k = 0; k < NS; ++k) sum1 += X[k] * mui[k], sum2 += X[k] / mui[k];
-    lam = 0.5 * (sum1 + 1 / sum2);
+    lam = MT(0.5) * (sum1 + 1 / sum2);
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        const double s = sqsqT * dot5(lgT, lgT2, lgT3, lgT4, visc + 5 * n);
+        const MT s = sqsqT * dot5t<MT>(lgT, lgT2, lgT3, lgT4, visc + 5 * n);
         mui[n] = s * s;
-        row[n] = 0.0;
+        row[n] = 0;
     }
-    double rmu[NS];
+    MT rmu[NS];
 #pragma unroll
     for (int n = 0; n < NS; ++n) rmu[n] = 1 / mui[n];
 #pragma unroll
@@ -548,42 +566,41 @@ __device__ __forceinline__ void mixture_properties_pairs(double T, double P, con
 #pragma unroll
         for (int l = 0; l < n; ++l) {
             const int i = n * NS + l;
-            const double vr = mui[n] * rmu[l];  // μ_n / μ_l
-            const double f1 = 1 + sqrt(vr * pw[NS * NS + i]);
-            const double t = f1 * f1 * pw[2 * NS * NS + i];
+            const MT vr = mui[n] * rmu[l];  // μ_n / μ_l
+            const MT f1 = 1 + sqrt(vr * pw[NS * NS + i]);
+            const MT t = f1 * f1 * pw[2 * NS * NS + i];
             row[n] += X[l] * t;                                 // W[n][l]
             row[l] += X[n] * (t * (mui[l] * rmu[n]) * pw[i]);  // W[l][n] = t / (vr wr)
         }
-        row[n] += X[n] * 1.0;  // W[n][n]
+        row[n] += X[n] * MT(1);  // W[n][n]
     }
     mu = 0;
 #pragma unroll
     for (int n = 0; n < NS; ++n) mu += X[n] * mui[n] / row[n];
 #pragma unroll
-    for (int n = 0; n < NS; ++n) row[n] = 0.0;  // now Σ_{m≠n} X[m] / Dbin[n][m]
+    for (int n = 0; n < NS; ++n) row[n] = 0;  // now Σ_{m≠n} X[m] / Dbin[n][m]
 #pragma unroll
     for (int n = 0; n < NS; ++n)
 #pragma unroll
         for (int m = n + 1; m < NS; ++m) {
-            const double t = T * sqT * dot5(lgT, lgT2, lgT3, lgT4, bin + 5 * (m + NS * n));
-            const double rt = 1 / t;
+            const MT t = T * sqT * dot5t<MT>(lgT, lgT2, lgT3, lgT4, bin + 5 * (m + NS * n));
+            const MT rt = 1 / t;
             row[n] += X[m] * rt;
             row[m] += X[n] * rt;
         }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        const double s = row[n] * P;
-        Dk[n] = (1 - X[n]) / (s + kEps);
+        const MT s = row[n] * P;
+        Dk[n] = (1 - X[n]) / (s + MT(kEps));
     }
 }
 
 // The reference's mixture kernel at one point with law 2 (thermo.jl:371-403): Y = max(ρi/ρ, 0)
-// with ρ = max(Q_ρ, eps), X from Y (Y2X, thermo.jl:38-52), then mixtureProperties.  The fused
-// stage stores the result as μ, λ, D_0 .. D_{NS-1}.
-// pw: the block's wilke_pairs_fill table.
-template <int NS>
+// with ρ = max(Q_ρ, eps), X from Y (Y2X, thermo.jl:38-52), then mixtureProperties in MT.  The
+// fused stage stores the result as μ, λ, D_0 .. D_{NS-1}.  mt: the block's MixTables.
+template <int NS, typename MT>
 __device__ __forceinline__ void mixture_point(const FlameThermo &th, const FlameTransport &tr,
-                                              const double *pw, double T, double P,
+                                              const MixTables<NS, MT> &mt, double T, double P,
                                               double rho_raw, const double *r, double &mu,
                                               double &lam, double *Dk) {
     const double rhoinv = 1 / jmax(rho_raw, kEps);
@@ -594,7 +611,17 @@ __device__ __forceinline__ void mixture_point(const FlameThermo &th, const Flame
     const double yowinv = 1 / yow;
 #pragma unroll
     for (int n = 0; n < NS; ++n) X[n] = X[n] / th.mw[n] * yowinv;
-    mixture_properties_pairs<NS>(T, P, X, pw, tr.poly, Dk, lam, mu);
+    if constexpr (sizeof(MT) == 8) {
+        mixture_properties_pairs<NS, double>(T, P, X, mt.pw, tr.poly, Dk, lam, mu);
+    } else {
+        MT Xm[NS], Dm[NS], lm, mm;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) Xm[n] = MT(X[n]);
+        mixture_properties_pairs<NS, MT>(MT(T), MT(P), Xm, mt.pw, mt.poly, Dm, lm, mm);
+        lam = lm, mu = mm;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) Dk[n] = Dm[n];
+    }
 }
 
 // An NVTX range over a host-side scope (stage launches show up by name in Nsight timelines).

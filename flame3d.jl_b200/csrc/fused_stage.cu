@@ -562,15 +562,15 @@ template <int NS, typename QT>
 __global__ void k_transport_mix(int np, const QT *__restrict__ Q, const double *__restrict__ ri,
                                 QT *__restrict__ To, const FlameThermo th,
                                 const FlameTransport tr) {
-    __shared__ double pw[3 * NS * NS];
-    wilke_pairs_fill<NS>(th, pw);
+    __shared__ MixTables<NS, QT> mt;
+    mix_tables_fill<NS, QT>(th, tr, mt);
     __syncthreads();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= np) return;
     double r[NS], Dk[NS], mu, lam;
 #pragma unroll
     for (int n = 0; n < NS; ++n) r[n] = ri[c + n * np];
-    mixture_point<NS>(th, tr, pw, double(Q[c + 5 * np]), double(Q[c + 4 * np]), double(Q[c]), r,
+    mixture_point<NS, QT>(th, tr, mt, double(Q[c + 5 * np]), double(Q[c + 4 * np]), double(Q[c]), r,
                       mu, lam, Dk);
     To[c] = QT(mu), To[c + np] = QT(lam);
 #pragma unroll

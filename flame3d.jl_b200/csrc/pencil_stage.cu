@@ -442,10 +442,11 @@ __device__ __forceinline__ void species_point_phase(const Args<QT> &A, CT *S, in
 
 // ---- last sweep: div, RK3 combination, c2Prim, transport, ghost images of one cell.
 // LAW2: the mixture-averaged transport, written as μ, λ, D_0 .. D_{NS-1}.
-// pw: the block's wilke_pairs_fill table (LAW2 only).
+// mt: the block's MixTables (LAW2 only).
 template <int NS, typename QT, bool LAW2 = false>
 __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, int gy, int gz,
-                                            const double *rhs, const double *pw = nullptr) {
+                                            const double *rhs,
+                                            const MixTables<NS, QT> *mt = nullptr) {
     const int np = A.np;
     const double Jact = A.met[9][g] * A.dt;
     double Uc[5], r[NS];
@@ -500,7 +501,7 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
         }
     }
     if constexpr (LAW2) {  // the next stage's mixture kernel (thermo.jl:371-403), per cell
-        mixture_point<NS>(A.th, A.tr, pw, Tn, p, rho, r, mu, lam, Dk);
+        mixture_point<NS, QT>(A.th, A.tr, *mt, Tn, p, rho, r, mu, lam, Dk);
         D = Dk[0];
     }
     const double qv[7] = {rho, u, v, w, p, Tn, ei};
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_co
 // The stage's finish for configuration 4: one thread per interior cell, x fastest, with the
 // complete right-hand side already in R (the x sweep summed it).
 template <int NS, typename QT, bool LAW2>
-__device__ __forceinline__ void finish_thread(const Args<QT> &A, const double *pw) {
+__device__ __forceinline__ void finish_thread(const Args<QT> &A, const MixTables<NS, QT> *mt) {
     const int c = blockIdx.x * 128 + threadIdx.x;
     if (c >= A.nx * A.ny * A.nz) return;
     const int x = c % A.nx, y = (c / A.nx) % A.ny, z = c / (A.nx * A.ny);
@@ -615,7 +616,7 @@ __device__ __forceinline__ void finish_thread(const Args<QT> &A, const double *p
     double rhs[5 + NS];
 #pragma unroll
     for (int n = 0; n < 5 + NS; ++n) rhs[n] = A.R[g + n * A.np];
-    finish_cell<NS, QT, LAW2>(A, g, gx, gy, gz, rhs, pw);
+    finish_cell<NS, QT, LAW2>(A, g, gx, gy, gz, rhs, mt);
 }
 
 template <int NS, typename QT>
@@ -628,10 +629,10 @@ __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT>
 // it runs faster.  A separate kernel, so that the bound does not touch the other laws' finish.
 template <int NS, typename QT>
 __global__ void __launch_bounds__(128, 4) k_finish_mix(const __grid_constant__ Args<QT> A) {
-    __shared__ double pw[3 * NS * NS];
-    wilke_pairs_fill<NS>(A.th, pw);
+    __shared__ MixTables<NS, QT> mt;
+    mix_tables_fill<NS, QT>(A.th, A.tr, mt);
     __syncthreads();
-    finish_thread<NS, QT, true>(A, pw);
+    finish_thread<NS, QT, true>(A, &mt);
 }
 
 // Columns per block of the staged y / z sweeps.  Single precision: 16 consecutive x columns, so

@@ -316,8 +316,8 @@ typedef struct FlameStageBuffers {
 } FlameStageBuffers;
 
 /* stage in {1,2,3}; precision 0 = plain FP64, 1 = mixed (FP32 storage of Q and transport, FP32
- * split / reconstruction with its WENO-Z weights / viscous fluxes; FP64 conserved accumulation,
- * metrics and Newton temperature).  No reference counterpart: it replaces the launch sequence
+ * split / reconstruction with its WENO-Z weights / viscous fluxes and, with law 2, the mixture
+ * rule; FP64 conserved accumulation, metrics and Newton temperature).  No reference counterpart: it replaces the launch sequence
  * of solver.jl:298-326. */
 int flame_rk_stage(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                    const FlameStageBuffers *b, const FlameMetrics *m, const FlameThermo *thermo,
