@@ -88,8 +88,9 @@ struct Slots {
 };
 
 // Slots of the species sweep (PART 2): only what the species fluxes and the enthalpy
-// diffusion term of the energy flux read.
-template <int NS>
+// diffusion term of the energy flux read.  MIXD (law 2): D holds D_0 and DK the other species'
+// D_1 .. D_{NS-1}.
+template <int NS, bool MIXD = false>
 struct SpSlots {
     static constexpr int FP = 0;                // F+ sp (NS), F- sp (NS)
     static constexpr int SPP = 0, SPM = NS;
@@ -101,14 +102,15 @@ struct SpSlots {
     static constexpr int Y = PHI + 1;           // NS
     static constexpr int DY1 = Y + NS;          // NS
     static constexpr int DY2 = DY1 + NS;        // NS
-    static constexpr int N = DY2 + NS;          // 5 NS + 14
+    static constexpr int DK = DY2 + NS;         // NS - 1 (MIXD only)
+    static constexpr int N = DK + (MIXD ? NS - 1 : 0);  // 5 NS + 14 (+ NS - 1)
     static constexpr int G = FP;                // NS species fluxes + the energy term
 };
 
 // PART 0: the whole face flux; PART 2: the species fluxes and the enthalpy-diffusion term of the
 // energy flux only (the flow part then runs as the NS = 0 instance of the same sweep).
-template <int NS, int PART>
-using SlotsOf = std::conditional_t<PART == 2, SpSlots<NS>, Slots<NS>>;
+template <int NS, int PART, bool MIXD = false>
+using SlotsOf = std::conditional_t<PART == 2, SpSlots<NS, MIXD>, Slots<NS>>;
 
 template <int NS, typename CT, int WPB>
 constexpr size_t smem_bytes() {
@@ -290,7 +292,7 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 template <int DIR, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G,
                                            const QT *Dk, int dstep) {
-    using SL = SlotsOf<NS, PART>;
+    using SL = SlotsOf<NS, PART, MIXD>;
     constexpr int GS = PART == 2 ? 0 : 5;  // G index of species 0
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
     const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
@@ -320,7 +322,10 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
     const CT rhoD1 = (DL + DR) * rho;  // viscous.jl:473 (no 1/2, as the reference)
     auto diffusion = [&](int n, CT &Vx, CT &Vy, CT &Vz) {
         CT rhoDi = rhoD1;
-        if constexpr (MIXD) {
+        if constexpr (MIXD && PART == 2) {  // staged with the species slots
+            constexpr int dk = SpSlots<NS, true>::DK;
+            if (n > 0) rhoDi = (SV(dk + n - 1, lm) + SV(dk + n - 1, l)) * rho;
+        } else if constexpr (MIXD) {  // the x sweep: coalesced loads
             const QT *dn = Dk + (size_t)n * A.np;
             rhoDi = (CT(dn[-dstep]) + CT(dn[0])) * rho;
         }
@@ -396,9 +401,9 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
 }
 
 // ---- phase A of the species sweep: the species slots of one point.
-template <int DIR, int NS, typename QT, typename CT>
+template <int DIR, int NS, typename QT, typename CT, bool MIXD = false>
 __device__ __forceinline__ void species_point_phase(const Args<QT> &A, CT *S, int l, int g) {
-    using SL = SpSlots<NS>;
+    using SL = SpSlots<NS, MIXD>;
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
     const int np = A.np;
     const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
@@ -427,6 +432,10 @@ __device__ __forceinline__ void species_point_phase(const Args<QT> &A, CT *S, in
 #pragma unroll
     for (int m = 0; m < 10; ++m) SV(SL::MET + m) = mv[m];
     SV(SL::D) = CT(A.Ti[g + 2 * np]);
+    if constexpr (MIXD) {
+#pragma unroll
+        for (int n = 1; n < NS; ++n) SV(SL::DK + n - 1) = CT(A.Ti[g + (2 + n) * np]);
+    }
     SV(SL::RHO) = rho;
     SV(SL::T) = CT(Q[g + 5 * np]);
     SV(SL::PHI) = CT(A.aux[g]);
@@ -651,10 +660,10 @@ constexpr int staged_cols(int ns, size_t csz) {
     return (csz == 8 && ns > 0) ? 8 : (csz * slots_of(ns) * 33 * 16 <= 200 * 1024 ? 16 : 8);
 }
 
-template <int NS, typename CT, int PART = 0>
+template <int NS, typename CT, int PART = 0, bool MIXD = false>
 struct Staged {
     static_assert(Slots<NS>::N == slots_of(NS), "slots_of must follow Slots");
-    static constexpr int NSLOT = SlotsOf<NS, PART>::N;
+    static constexpr int NSLOT = SlotsOf<NS, PART, MIXD>::N;
     static constexpr int STRIDE = NSLOT * 32 + 1;  // padded column region (bank spread)
     // (the species sweep in 8-column blocks capped at three per SM measured 7-12 % slower in
     // mixed precision: the register cap spills)
@@ -669,8 +678,9 @@ struct Staged {
 // PASS 0 writes R, PASS 1 adds to it.
 template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsigned char *smem_raw) {
-    constexpr int COLS = Staged<NS, CT, PART>::COLS, STRIDE = Staged<NS, CT, PART>::STRIDE;
-    using SL = SlotsOf<NS, PART>;
+    constexpr int COLS = Staged<NS, CT, PART, MIXD>::COLS;
+    constexpr int STRIDE = Staged<NS, CT, PART, MIXD>::STRIDE;
+    using SL = SlotsOf<NS, PART, MIXD>;
     constexpr int NG_OUT = PART == 2 ? NS + 1 : 5 + NS;  // face values a lane produces
     CT *base = reinterpret_cast<CT *>(smem_raw);
     const int n_along = DIR == 1 ? A.ny : A.nz;
@@ -702,7 +712,8 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
         const int gy = DIR == 1 ? ga : c2 + A.ng;
         const int gz = DIR == 1 ? c2 + A.ng : ga;
         if constexpr (PART == 2)
-            species_point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
+            species_point_phase<DIR, NS, QT, CT, MIXD>(A, base + cx * STRIDE, l,
+                                                       gx + A.sy * gy + A.sz * gz);
         else
             point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
     }
@@ -750,7 +761,7 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
 }
 
 template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
-__global__ void __launch_bounds__(Staged<NS, CT, PART>::COLS * 32)
+__global__ void __launch_bounds__(Staged<NS, CT, PART, MIXD>::COLS * 32)
     k_pencil_staged(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     staged_block<DIR, PASS, NS, QT, CT, PART, MIXD>(A, blockIdx.x, smem_raw);
@@ -849,7 +860,7 @@ int set_smem(K kernel, size_t sm, bool *done) {
 
 template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 int launch_staged(const Args<QT> &A, cudaStream_t s) {
-    using ST = Staged<NS, CT, PART>;
+    using ST = Staged<NS, CT, PART, MIXD>;
     constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
     static bool done[64] = {};
     if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD>, sm, done)) return e;
