@@ -2,7 +2,8 @@
 
 * launch sequence (1:1 kernels, -fmad=false): agrees with the oracle to 1e-14 relative L2
   (only pow() in the transport law differs from libm);
-* fused one-launch stage, plain FP64: ≤ 1e-12 relative L2 per field (the north-star bound);
+* fused one-launch stage, plain FP64: ≤ 1e-12 relative L2 per field (the bound the fused
+  path is held to);
 * fused stage, mixed precision: ≤ 1e-5 relative L2 in ρ, ρu, ρE after several steps.
 """
 from __future__ import annotations
