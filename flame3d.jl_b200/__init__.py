@@ -8,12 +8,13 @@ There is no CPU fallback: without the library or a GPU every entry point raises.
 from .abi import (FLAME_MAX_NS, FLAME_NG, FlameError, FlameGrid, FlameMetrics,  # noqa: F401
                   FlameStageBuffers, FlameThermo, FlameTransport, header_symbols, load_library)
 from .cases import (Case, Thermo, Transport, curvilinear_jet, ideal_air,  # noqa: F401
-                    mixing_layer, random_curvilinear, synthetic_species, taylor_green)
+                    inflow_jet, mixing_layer, random_curvilinear, synthetic_species,
+                    taylor_green)
 
 __all__ = ["FlameError", "FlameGrid", "FlameMetrics", "FlameStageBuffers", "FlameThermo",
            "FlameTransport", "Case", "Thermo", "Transport", "load_library", "header_symbols",
            "taylor_green", "curvilinear_jet", "mixing_layer", "random_curvilinear",
-           "ideal_air", "synthetic_species"]
+           "inflow_jet", "ideal_air", "synthetic_species"]
 
 
 def batch_module():

@@ -66,6 +66,11 @@ class FlameReactions(C.Structure):
 class FlameMetrics(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in METRIC_NAMES]
 
+    def args(self) -> tuple:
+        """The ten pointers in the reference's argument order (dξdx … dζdz, J), for the entry
+        points that take them as separate arguments."""
+        return tuple(getattr(self, n) for n in METRIC_NAMES)
+
 
 class FlameStageBuffers(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("U", "Un", "Q_in", "Q_out", "rhoi_in", "rhoi_out",
@@ -87,6 +92,7 @@ TH = C.POINTER(FlameThermo)
 TR = C.POINTER(FlameTransport)
 I = C.c_int
 D = C.c_double
+MET10 = [P] * 10  # the nine metric cofactors and J as separate arrays (viscous.jl:1, 430)
 
 SIGNATURES = {
     "flame_shockSensor": [G, S, P, P],
@@ -95,12 +101,12 @@ SIGNATURES = {
     "flame_WENO_x": [G, S, P, P, P, P, I, P],
     "flame_WENO_y": [G, S, P, P, P, P, I, P],
     "flame_WENO_z": [G, S, P, P, P, P, I, P],
-    "flame_viscousFlux_x": [G, S, P, P, M, P, P, P, P],
-    "flame_viscousFlux_y": [G, S, P, P, M, P, P, P, P],
-    "flame_viscousFlux_z": [G, S, P, P, M, P, P, P, P],
-    "flame_specViscousFlux_x": [G, S, P, P, P, M, P, P, TH, P],
-    "flame_specViscousFlux_y": [G, S, P, P, P, M, P, P, TH, P],
-    "flame_specViscousFlux_z": [G, S, P, P, P, M, P, P, TH, P],
+    "flame_viscousFlux_x": [G, S, P, P, *MET10, P, P, P, P],
+    "flame_viscousFlux_y": [G, S, P, P, *MET10, P, P, P, P],
+    "flame_viscousFlux_z": [G, S, P, P, *MET10, P, P, P, P],
+    "flame_specViscousFlux_x": [G, S, P, P, P, *MET10, P, P, TH, P],
+    "flame_specViscousFlux_y": [G, S, P, P, P, *MET10, P, P, TH, P],
+    "flame_specViscousFlux_z": [G, S, P, P, P, *MET10, P, P, TH, P],
     "flame_div": [G, S, P, P, P, P, P, P, P, D, P, P],
     "flame_divSpecs": [G, S, P, P, P, P, P, P, P, D, P, P],
     "flame_linComb": [G, S, P, P, I, D, D, P],
@@ -120,12 +126,13 @@ SIGNATURES = {
     "flame_check_finite": [G, S, P, I, P],
     "flame_eval_gpu": [G, S, P, P, P, D, TH, C.POINTER(FlameReactions), P, D],
     "flame_eval_gpu_stiff": [G, S, P, P, P, D, TH, C.POINTER(FlameReactions), P, D, I],
-    "flame_flowAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, P, P],
-    "flame_specAdvance": [G, S, P, P, P, P, P, P, P, P, P, P, P, M, D, P, P, P, P, P, TH, P],
+    "flame_flowAdvance": [G, S, *[P] * 10, *MET10, D, P, P, P, P, P, P, P],
+    "flame_specAdvance": [G, S, *[P] * 11, *MET10, D, P, P, P, P, P, TH, P],
     "flame_rk_stage": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
     "flame_rk_stage_tiled": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I, I],
     "flame_rk_stage_noalloc": [G, S, I, D, C.POINTER(FlameStageBuffers), M, TH, TR, I],
     "flame_transport": [G, S, P, P, P, TH, TR, I],
+    "flame_transport_boundary": [G, S, P, P, P, TH, TR, I],
     "flame_stage_scratch_bytes": [G, I],
     "flame_batch_workspace_bytes": [C.POINTER(FlameCaseDesc), I, I],
     "flame_batch_create": [C.POINTER(C.c_void_p), C.POINTER(FlameCaseDesc), I, I, P, C.c_size_t,

@@ -321,6 +321,9 @@ class Case:
     steps: int = 1
     periodic: int = 7
     info: dict = field(default_factory=dict)
+    # non-periodic cases: the inflow state of the reference's fills (FlameInflow), used by
+    # fill_x / fill_z at the x-low and z-low boundaries (boundary.jl:1-137)
+    inflow: object = None
 
     @property
     def ns(self) -> int:
@@ -549,7 +552,51 @@ def random_curvilinear(n: int = 16, ns: int = 1, seed: int = 11, amp: float = 0.
                    T, Ys, cfl, 1, {"seed": seed})
 
 
+def inflow_jet(nx: int = 32, ny: int = 16, nz: int = 16, ns: int = 5, seed: int = 12,
+               amp: float = 0.1, cfl: float = 0.5) -> Case:
+    """The reference's own boundary conditions (boundary.jl:1-191, solver.jl:321-325): not
+    periodic; supersonic inflow at the x-low and z-low boundaries with the state fill_x / fill_z
+    hard-code (79.8 Pa, 270.65 K, 1000 m/s along x, Y_2 = 0.233, Y_5 = 0.767), zero-gradient
+    copies elsewhere.  The initial field is that free stream (boundary.jl:281-324) on the wavy
+    mapping (scaled to a 1 m box), with a hot, fast round jet of species 1 along x through the
+    middle (diameter 0.25, 900 K, u = 2000 m/s, Y_1 = 0.3), seeded 2 % velocity and pressure
+    noise and a 1.6x pressure jump at two thirds of x, so all hybrid branches occur.  Synthetic species (`ns` >= 5).  Ghosts are given
+    zero-gradient copies here; the device and the oracle replace them with the reference's
+    fills before the first stage, as solver.jl:192-200 does."""
+    thermo = synthetic_species(max(ns, 5), 3).subset(ns)
+    inflow = reference_inflow(ns)
+    metrics, xyz = wavy_metrics(nx, ny, nz, amp)
+    rng = np.random.default_rng(seed)
+    kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    X, Y, Z = xyz(ii.astype(float), jj.astype(float), kk.astype(float))
+    r = np.sqrt((Y - 0.5) ** 2 + (Z - 0.5) ** 2)
+    f = 0.5 * (1 + np.tanh((0.125 - r) / 0.02))
+    Yair = np.array([inflow.Y[n] for n in range(ns)])
+    Yjet = 0.7 * Yair
+    Yjet[0] += 0.3
+    Ys = (1 - f)[None] * Yair[:, None, None, None] + f[None] * Yjet[:, None, None, None]
+    T = inflow.T + (900.0 - inflow.T) * f
+    p = inflow.P * (1 + 0.02 * rng.uniform(-1, 1, T.shape))
+    p[:, :, 2 * nx // 3:] *= 1.6  # a pressure jump across x = 2/3: minmod faces
+    u = inflow.u + 1000.0 * f + 20.0 * rng.uniform(-1, 1, T.shape)
+    v = 20.0 * rng.uniform(-1, 1, T.shape)
+    w = 20.0 * rng.uniform(-1, 1, T.shape)
+    Wmix = 1.0 / np.sum(Ys / thermo.mw[:, None, None, None], axis=0)
+    rho = p * Wmix / (thermo.Ru * T)
+    tr = Transport(law=1, mu_ref=1.8e-5, T_ref=300.0, exponent=0.7, Pr=0.71)
+    c = _finish(f"inflowjet{nx}x{ny}x{nz}_ns{ns}", nx, ny, nz, thermo, tr, metrics, rho, u, v, w,
+                T, Ys, cfl, 1, {"seed": seed, "bc": "reference inflow / zero gradient"})
+    # zero-gradient ghosts in place of the periodic images _finish made
+    sl = (slice(None), slice(NG, NG + nz), slice(NG, NG + ny), slice(NG, NG + nx))
+    pad = ((0, 0), (NG, NG), (NG, NG), (NG, NG))
+    c.Q = np.ascontiguousarray(np.pad(c.Q[sl], pad, mode="edge"))
+    c.rhoi = np.ascontiguousarray(np.pad(c.rhoi[sl], pad, mode="edge"))
+    c.periodic = 0
+    c.inflow = inflow
+    return c
+
+
 def case_by_name(name: str, **kw) -> Case:
     table = {"tgv": taylor_green, "jet": curvilinear_jet, "mixing": mixing_layer,
-             "random": random_curvilinear}
+             "random": random_curvilinear, "inflow": inflow_jet}
     return table[name](**kw)

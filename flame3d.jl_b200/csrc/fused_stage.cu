@@ -69,6 +69,7 @@ struct Layout {
 template <typename QT>
 struct Args {
     int nx, ny, nz, ng, tx, ty, tz, np, sy, sz;
+    int per;  // periodic axes (FlameGrid::periodic): ghost images are written on these only
     int stage;
     double dt, ca, cb;  // RK3 combination U = ca*U + cb*Un (stages 2, 3)
     double *U, *Un;
@@ -498,18 +499,25 @@ struct Tile {
             transport_point<NS>(A.th, A.tr, Tn, rho, r, mu, lam, D);
             const double qv[7] = {rho, u, v, w, p, Tn, ei};
             const double tv[3] = {mu, lam, D};
-            // the cell and its periodic ghost images (new: the reference fills ghosts with
-            // case-specific kernels, boundary.jl:1-191)
+            // the cell and its ghost images along the periodic axes (new: the reference fills
+            // ghosts with case-specific kernels, boundary.jl:1-191, which the caller runs after
+            // the stage for the other axes)
             const int gx = ix + ng, gy = iy + ng, gz = iz + ng;
             // up to two images per axis: an axis shorter than 2 NG has cells near both ends
-    int ox[3] = {0, 0, 0}, oy[3] = {0, 0, 0}, oz[3] = {0, 0, 0};
+            int ox[3] = {0, 0, 0}, oy[3] = {0, 0, 0}, oz[3] = {0, 0, 0};
             int nxo = 1, nyo = 1, nzo = 1;
-            if (gx < 2 * ng) ox[nxo++] = A.nx;
-            if (gx >= A.nx) ox[nxo++] = -A.nx;
-            if (gy < 2 * ng) oy[nyo++] = A.ny;
-            if (gy >= A.ny) oy[nyo++] = -A.ny;
-            if (gz < 2 * ng) oz[nzo++] = A.nz;
-            if (gz >= A.nz) oz[nzo++] = -A.nz;
+            if (A.per & 1) {
+                if (gx < 2 * ng) ox[nxo++] = A.nx;
+                if (gx >= A.nx) ox[nxo++] = -A.nx;
+            }
+            if (A.per & 2) {
+                if (gy < 2 * ng) oy[nyo++] = A.ny;
+                if (gy >= A.ny) oy[nyo++] = -A.ny;
+            }
+            if (A.per & 4) {
+                if (gz < 2 * ng) oz[nzo++] = A.nz;
+                if (gz >= A.nz) oz[nzo++] = -A.nz;
+            }
             for (int c = 0; c < nzo; ++c)
                 for (int b = 0; b < nyo; ++b)
                     for (int a = 0; a < nxo; ++a) {
@@ -543,12 +551,28 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage(const __grid_constant_
     t.epilogue(acc);
 }
 
-// Transport of every ghosted point of a state (used once to start the fused stage loop).
+// The points whose transport a ghost fill can invalidate: with `on` set, a ghosted point is
+// taken when, on an axis that is not periodic, it is a ghost or the first or last interior
+// plane (the planes the reference's fills overwrite, boundary.jl:1-176); otherwise every point.
+struct Shell {
+    int on, tx, ty, nx, ny, nz, ng, per;
+    __device__ __forceinline__ bool take(int c) const {
+        if (!on) return true;
+        const int gx = c % tx, gy = (c / tx) % ty, gz = c / (tx * ty);
+        const auto edge = [this](int g, int n) { return g <= ng || g >= n + ng - 1; };
+        return (!(per & 1) && edge(gx, nx)) || (!(per & 2) && edge(gy, ny)) ||
+               (!(per & 4) && edge(gz, nz));
+    }
+};
+
+// Transport of the ghosted points of a state (every point once, to start the fused stage loop;
+// the boundary shell after a ghost fill).
 template <int NS, typename QT>
 __global__ void k_transport(int np, const QT *__restrict__ Q, const double *__restrict__ ri,
-                            QT *__restrict__ To, const FlameThermo th, const FlameTransport tr) {
+                            QT *__restrict__ To, const FlameThermo th, const FlameTransport tr,
+                            const Shell sh) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= np) return;
+    if (c >= np || !sh.take(c)) return;
     double r[NS];
 #pragma unroll
     for (int n = 0; n < NS; ++n) r[n] = ri[c + n * np];
@@ -561,12 +585,12 @@ __global__ void k_transport(int np, const QT *__restrict__ Q, const double *__re
 template <int NS, typename QT>
 __global__ void k_transport_mix(int np, const QT *__restrict__ Q, const double *__restrict__ ri,
                                 QT *__restrict__ To, const FlameThermo th,
-                                const FlameTransport tr) {
+                                const FlameTransport tr, const Shell sh) {
     __shared__ MixTables<NS, QT> mt;
     mix_tables_fill<NS, QT>(th, tr, mt);
     __syncthreads();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= np) return;
+    if (c >= np || !sh.take(c)) return;
     double r[NS], Dk[NS], mu, lam;
 #pragma unroll
     for (int n = 0; n < NS; ++n) r[n] = ri[c + n * np];
@@ -585,6 +609,7 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
     A.tx = g.nx + 2 * g.ng, A.ty = g.ny + 2 * g.ng, A.tz = g.nz + 2 * g.ng;
     A.np = A.tx * A.ty * A.tz;
     A.sy = A.tx, A.sz = A.tx * A.ty;
+    A.per = g.periodic & 7;
     A.stage = stage;
     A.dt = dt;
     A.ca = stage == 2 ? 0.25 : 2.0 / 3.0;
@@ -659,15 +684,15 @@ int dispatch_tile(int tile, int ns, const FlameGrid &g, cudaStream_t s, int stag
 
 template <typename QT>
 int transport_ns(int ns, int np, cudaStream_t s, const void *Q, const double *ri, void *To,
-                 const FlameThermo &th, const FlameTransport &tr) {
+                 const FlameThermo &th, const FlameTransport &tr, const Shell &sh) {
     const unsigned blocks = (unsigned)((np + 255) / 256);
     const QT *q = static_cast<const QT *>(Q);
     QT *t = static_cast<QT *>(To);
     switch (ns) {
-#define CASE(N)                                                                  \
-    case N:                                                                      \
-        if (tr.law == 2) k_transport_mix<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr); \
-        else k_transport<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr);    \
+#define CASE(N)                                                                              \
+    case N:                                                                                  \
+        if (tr.law == 2) k_transport_mix<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr, sh); \
+        else k_transport<N, QT><<<blocks, 256, 0, s>>>(np, q, ri, t, th, tr, sh);           \
         break;
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
@@ -680,33 +705,59 @@ int transport_ns(int ns, int np, cudaStream_t s, const void *Q, const double *ri
 }  // namespace flame
 
 namespace {
+// Every array of the stage must hold fewer than 2^31 elements (32-bit indices).  Extents are
+// widened to 64 bits and multiplied one at a time, so absurd extents cannot wrap into a small
+// product: before each multiplication the partial product is below 2^28 and the factor below
+// 2^32.
 int check_sizes(const FlameGrid *g, const char *what) {
-    const long long np = (long long)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
     const long long nv = g->ns > 10 ? g->ns : 10;
-    if (np * nv >= (1LL << 31))
-        return flame_fail(FLAME_EINVAL, "%s: %lld points x %lld fields exceeds 2^31 elements", what,
-                          np, nv);
+    const long long ext[3] = {(long long)g->nx + 2LL * g->ng, (long long)g->ny + 2LL * g->ng,
+                              (long long)g->nz + 2LL * g->ng};
+    long long np = 1;
+    for (long long e : ext) {
+        np *= e;
+        if (np * nv >= (1LL << 31))
+            return flame_fail(FLAME_EINVAL,
+                              "%s: %dx%dx%d cells with %lld fields exceed 2^31 elements per array",
+                              what, g->nx, g->ny, g->nz, nv);
+    }
     return FLAME_OK;
 }
 }  // namespace
 
+static int transport_call(const FlameGrid *g, flame_stream_t s, const void *Q,
+                          const double *rhoi, void *trans, const FlameThermo *th,
+                          const FlameTransport *tr, int precision, bool shell,
+                          const char *what) {
+    if (int e = flame_check_grid(g, what)) return e;
+    if (int e = check_sizes(g, what)) return e;
+    if (!Q || !rhoi || !trans || !th || !tr) return flame_fail(FLAME_EINVAL, "%s: NULL argument", what);
+    if (tr->law < 0 || tr->law > 2)
+        return flame_fail(FLAME_EINVAL, "%s: transport law %d unknown", what, tr->law);
+    if (tr->law == 2 && !tr->poly)
+        return flame_fail(FLAME_EINVAL, "%s: law 2 needs the polynomial fits (poly)", what);
+    const int np = (g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
+    const flame::fused::Shell sh{shell ? 1 : 0, g->nx + 2 * g->ng, g->ny + 2 * g->ng, g->nx,
+                                 g->ny, g->nz, g->ng, g->periodic & 7};
+    if (shell && sh.per == 7) return FLAME_OK;  // no axis is filled by the caller
+    if (precision == 0)
+        return flame::fused::transport_ns<double>(g->ns, np, s, Q, rhoi, trans, *th, *tr, sh);
+    if (precision == 1)
+        return flame::fused::transport_ns<float>(g->ns, np, s, Q, rhoi, trans, *th, *tr, sh);
+    return flame_fail(FLAME_EINVAL, "%s: precision=%d must be 0 or 1", what, precision);
+}
+
 extern "C" int flame_transport(const FlameGrid *g, flame_stream_t s, const void *Q,
                                const double *rhoi, void *trans, const FlameThermo *th,
                                const FlameTransport *tr, int precision) {
-    if (int e = flame_check_grid(g, "flame_transport")) return e;
-    if (int e = check_sizes(g, "flame_transport")) return e;
-    if (!Q || !rhoi || !trans || !th || !tr)
-        return flame_fail(FLAME_EINVAL, "flame_transport: NULL argument");
-    if (tr->law < 0 || tr->law > 2)
-        return flame_fail(FLAME_EINVAL, "flame_transport: transport law %d unknown", tr->law);
-    if (tr->law == 2 && !tr->poly)
-        return flame_fail(FLAME_EINVAL, "flame_transport: law 2 needs the polynomial fits (poly)");
-    const int np = (g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
-    if (precision == 0)
-        return flame::fused::transport_ns<double>(g->ns, np, s, Q, rhoi, trans, *th, *tr);
-    if (precision == 1)
-        return flame::fused::transport_ns<float>(g->ns, np, s, Q, rhoi, trans, *th, *tr);
-    return flame_fail(FLAME_EINVAL, "flame_transport: precision=%d must be 0 or 1", precision);
+    return transport_call(g, s, Q, rhoi, trans, th, tr, precision, false, "flame_transport");
+}
+
+extern "C" int flame_transport_boundary(const FlameGrid *g, flame_stream_t s, const void *Q,
+                                        const double *rhoi, void *trans, const FlameThermo *th,
+                                        const FlameTransport *tr, int precision) {
+    return transport_call(g, s, Q, rhoi, trans, th, tr, precision, true,
+                          "flame_transport_boundary");
 }
 
 extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int stage, double dt,
@@ -732,10 +783,6 @@ extern "C" int flame_rk_stage_tiled(const FlameGrid *g, flame_stream_t s, int st
         return flame_fail(FLAME_EUNSUPPORTED,
                           "flame_rk_stage: transport law 2 (per-species D_k) runs on the pencil "
                           "configurations 3-6, not on tile configuration %d", tile);
-    if ((g->periodic & 7) != 7)
-        return flame_fail(FLAME_EUNSUPPORTED,
-                          "flame_rk_stage: the fused stage needs a grid periodic in x, y and z; "
-                          "use the per-kernel entry points with the case's own ghost fill");
     if (g->nx < FLAME_NG || g->ny < FLAME_NG || g->nz < FLAME_NG)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage: extents must be >= %d", FLAME_NG);
     if (b->Q_in == b->Q_out || (const void *)b->rhoi_in == (const void *)b->rhoi_out ||

@@ -662,60 +662,75 @@ static bool metrics_ok(const FlameMetrics *m) {
            m->dzetadx && m->dzetady && m->dzetadz && m->J;
 }
 
+// The metric arguments of viscous.jl:1 and :430 (and of flowAdvance / specAdvance,
+// solver.jl:21,40): the nine J^-1-scaled cofactors in xi, eta, zeta order, then J.
+#define FLAME_METRIC_ARGS                                                                     \
+    const double *dxidx, const double *dxidy, const double *dxidz, const double *detadx,     \
+        const double *detady, const double *detadz, const double *dzetadx,                  \
+        const double *dzetady, const double *dzetadz, const double *J
+#define FLAME_METRIC_STRUCT \
+    FlameMetrics { dxidx, dxidy, dxidz, detadx, detady, detadz, dzetadx, dzetady, dzetadz, J }
+
 static int visc_dir(const FlameGrid *g, flame_stream_t s, int d, double *Fv, const double *Q,
-                    const FlameMetrics *m, const double *lambda, const double *mu,
+                    const FlameMetrics &m, const double *lambda, const double *mu,
                     const double *Fh, const int64_t *tag, const char *name) {
     if (int e = flame_check_grid(g, name)) return e;
-    if (!Fv || !Q || !lambda || !mu || !Fh || !metrics_ok(m))
+    if (!Fv || !Q || !lambda || !mu || !Fh || !metrics_ok(&m))
         return flame_fail(FLAME_EINVAL, "%s: NULL array", name);
     Dims D = make_dims(*g);
     FaceGeom f = face_geom(D, d);
-    k_viscousFlux<<<grid_for(f.fx, f.fy, f.fz), kBlock, 0, s>>>(D, f, d, Fv, Q, *m, lambda, mu,
+    k_viscousFlux<<<grid_for(f.fx, f.fy, f.fz), kBlock, 0, s>>>(D, f, d, Fv, Q, m, lambda, mu,
                                                                  Fh, tag);
     return flame_check_launch(name);
 }
 int flame_viscousFlux_x(const FlameGrid *g, flame_stream_t s, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        FLAME_METRIC_ARGS, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag) {
-    return visc_dir(g, s, 0, Fv, Q, m, lambda, mu, Fh, tag, "flame_viscousFlux_x");
+    return visc_dir(g, s, 0, Fv, Q, FLAME_METRIC_STRUCT, lambda, mu, Fh, tag,
+                    "flame_viscousFlux_x");
 }
 int flame_viscousFlux_y(const FlameGrid *g, flame_stream_t s, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        FLAME_METRIC_ARGS, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag) {
-    return visc_dir(g, s, 1, Fv, Q, m, lambda, mu, Fh, tag, "flame_viscousFlux_y");
+    return visc_dir(g, s, 1, Fv, Q, FLAME_METRIC_STRUCT, lambda, mu, Fh, tag,
+                    "flame_viscousFlux_y");
 }
 int flame_viscousFlux_z(const FlameGrid *g, flame_stream_t s, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        FLAME_METRIC_ARGS, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag) {
-    return visc_dir(g, s, 2, Fv, Q, m, lambda, mu, Fh, tag, "flame_viscousFlux_z");
+    return visc_dir(g, s, 2, Fv, Q, FLAME_METRIC_STRUCT, lambda, mu, Fh, tag,
+                    "flame_viscousFlux_z");
 }
 
 static int spec_dir(const FlameGrid *g, flame_stream_t s, int d, double *Fd, const double *Q,
-                    const double *Yi, const FlameMetrics *m, const double *Dk, double *Fh,
+                    const double *Yi, const FlameMetrics &m, const double *Dk, double *Fh,
                     const FlameThermo *th, const int64_t *tag, const char *name) {
     if (int e = flame_check_grid(g, name)) return e;
-    if (!Fd || !Q || !Yi || !Dk || !Fh || !th || !metrics_ok(m))
+    if (!Fd || !Q || !Yi || !Dk || !Fh || !th || !metrics_ok(&m))
         return flame_fail(FLAME_EINVAL, "%s: NULL argument", name);
     Dims D = make_dims(*g);
     FaceGeom f = face_geom(D, d);
-    k_specViscousFlux<<<grid_for(f.fx, f.fy, f.fz), kBlock, 0, s>>>(D, f, d, Fd, Q, Yi, *m, Dk,
+    k_specViscousFlux<<<grid_for(f.fx, f.fy, f.fz), kBlock, 0, s>>>(D, f, d, Fd, Q, Yi, m, Dk,
                                                                      Fh, *th, tag);
     return flame_check_launch(name);
 }
 int flame_specViscousFlux_x(const FlameGrid *g, flame_stream_t s, double *Fd, const double *Q,
-                            const double *Yi, const FlameMetrics *m, const double *Dk, double *Fh,
+                            const double *Yi, FLAME_METRIC_ARGS, const double *Dk, double *Fh,
                             const FlameThermo *th, const int64_t *tag) {
-    return spec_dir(g, s, 0, Fd, Q, Yi, m, Dk, Fh, th, tag, "flame_specViscousFlux_x");
+    return spec_dir(g, s, 0, Fd, Q, Yi, FLAME_METRIC_STRUCT, Dk, Fh, th, tag,
+                    "flame_specViscousFlux_x");
 }
 int flame_specViscousFlux_y(const FlameGrid *g, flame_stream_t s, double *Fd, const double *Q,
-                            const double *Yi, const FlameMetrics *m, const double *Dk, double *Fh,
+                            const double *Yi, FLAME_METRIC_ARGS, const double *Dk, double *Fh,
                             const FlameThermo *th, const int64_t *tag) {
-    return spec_dir(g, s, 1, Fd, Q, Yi, m, Dk, Fh, th, tag, "flame_specViscousFlux_y");
+    return spec_dir(g, s, 1, Fd, Q, Yi, FLAME_METRIC_STRUCT, Dk, Fh, th, tag,
+                    "flame_specViscousFlux_y");
 }
 int flame_specViscousFlux_z(const FlameGrid *g, flame_stream_t s, double *Fd, const double *Q,
-                            const double *Yi, const FlameMetrics *m, const double *Dk, double *Fh,
+                            const double *Yi, FLAME_METRIC_ARGS, const double *Dk, double *Fh,
                             const FlameThermo *th, const int64_t *tag) {
-    return spec_dir(g, s, 2, Fd, Q, Yi, m, Dk, Fh, th, tag, "flame_specViscousFlux_z");
+    return spec_dir(g, s, 2, Fd, Q, Yi, FLAME_METRIC_STRUCT, Dk, Fh, th, tag,
+                    "flame_specViscousFlux_z");
 }
 
 int flame_div(const FlameGrid *g, flame_stream_t s, double *U, const double *Fx, const double *Fy,
@@ -908,43 +923,47 @@ int flame_fill_periodic(const FlameGrid *g, flame_stream_t s, double *A, int nv)
 // solver.jl:22-38
 int flame_flowAdvance(const FlameGrid *g, flame_stream_t s, double *U, const double *Q, double *Fp,
                       double *Fm, double *Fx, double *Fy, double *Fz, double *Fvx, double *Fvy,
-                      double *Fvz, const FlameMetrics *m, double dt, const double *phi,
+                      double *Fvz, FLAME_METRIC_ARGS, double dt, const double *phi,
                       const double *lambda, const double *mu, const double *Fhx,
                       const double *Fhy, const double *Fhz, const int64_t *tag) {
-    if (!metrics_ok(m)) return flame_fail(FLAME_EINVAL, "flame_flowAdvance: NULL metrics");
+    const FlameMetrics m = FLAME_METRIC_STRUCT;
+    if (!metrics_ok(&m)) return flame_fail(FLAME_EINVAL, "flame_flowAdvance: NULL metrics");
     int e;
-    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, m->dxidx, m->dxidy, m->dxidz, tag))) return e;
+    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, dxidx, dxidy, dxidz, tag))) return e;
     if ((e = flame_WENO_x(g, s, Fx, phi, Fp, Fm, 5, tag))) return e;
-    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, m->detadx, m->detady, m->detadz, tag))) return e;
+    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, detadx, detady, detadz, tag))) return e;
     if ((e = flame_WENO_y(g, s, Fy, phi, Fp, Fm, 5, tag))) return e;
-    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, m->dzetadx, m->dzetady, m->dzetadz, tag))) return e;
+    if ((e = flame_fluxSplit(g, s, Q, Fp, Fm, dzetadx, dzetady, dzetadz, tag))) return e;
     if ((e = flame_WENO_z(g, s, Fz, phi, Fp, Fm, 5, tag))) return e;
-    if ((e = flame_viscousFlux_x(g, s, Fvx, Q, m, lambda, mu, Fhx, tag))) return e;
-    if ((e = flame_viscousFlux_y(g, s, Fvy, Q, m, lambda, mu, Fhy, tag))) return e;
-    if ((e = flame_viscousFlux_z(g, s, Fvz, Q, m, lambda, mu, Fhz, tag))) return e;
-    return flame_div(g, s, U, Fx, Fy, Fz, Fvx, Fvy, Fvz, dt, m->J, tag);
+    if ((e = visc_dir(g, s, 0, Fvx, Q, m, lambda, mu, Fhx, tag, "flame_viscousFlux_x"))) return e;
+    if ((e = visc_dir(g, s, 1, Fvy, Q, m, lambda, mu, Fhy, tag, "flame_viscousFlux_y"))) return e;
+    if ((e = visc_dir(g, s, 2, Fvz, Q, m, lambda, mu, Fhz, tag, "flame_viscousFlux_z"))) return e;
+    return flame_div(g, s, U, Fx, Fy, Fz, Fvx, Fvy, Fvz, dt, J, tag);
 }
 
 // solver.jl:40-56
 int flame_specAdvance(const FlameGrid *g, flame_stream_t s, double *rhoi, const double *Q,
                       const double *Yi, double *Fpi, double *Fmi, double *Fxi, double *Fyi,
-                      double *Fzi, double *Fdx, double *Fdy, double *Fdz, const FlameMetrics *m,
+                      double *Fzi, double *Fdx, double *Fdy, double *Fdz, FLAME_METRIC_ARGS,
                       double dt, const double *phi, const double *Dk, double *Fhx, double *Fhy,
                       double *Fhz, const FlameThermo *th, const int64_t *tag) {
-    if (!metrics_ok(m)) return flame_fail(FLAME_EINVAL, "flame_specAdvance: NULL metrics");
+    const FlameMetrics m = FLAME_METRIC_STRUCT;
+    if (!metrics_ok(&m)) return flame_fail(FLAME_EINVAL, "flame_specAdvance: NULL metrics");
     const int ns = g ? g->ns : 0;
     int e;
-    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, m->dxidx, m->dxidy, m->dxidz, tag))) return e;
+    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, dxidx, dxidy, dxidz, tag))) return e;
     if ((e = flame_WENO_x(g, s, Fxi, phi, Fpi, Fmi, ns, tag))) return e;
-    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, m->detadx, m->detady, m->detadz, tag))) return e;
+    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, detadx, detady, detadz, tag))) return e;
     if ((e = flame_WENO_y(g, s, Fyi, phi, Fpi, Fmi, ns, tag))) return e;
-    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, m->dzetadx, m->dzetady, m->dzetadz, tag)))
-        return e;
+    if ((e = flame_split(g, s, rhoi, Q, Fpi, Fmi, dzetadx, dzetady, dzetadz, tag))) return e;
     if ((e = flame_WENO_z(g, s, Fzi, phi, Fpi, Fmi, ns, tag))) return e;
-    if ((e = flame_specViscousFlux_x(g, s, Fdx, Q, Yi, m, Dk, Fhx, th, tag))) return e;
-    if ((e = flame_specViscousFlux_y(g, s, Fdy, Q, Yi, m, Dk, Fhy, th, tag))) return e;
-    if ((e = flame_specViscousFlux_z(g, s, Fdz, Q, Yi, m, Dk, Fhz, th, tag))) return e;
-    return flame_divSpecs(g, s, rhoi, Fxi, Fyi, Fzi, Fdx, Fdy, Fdz, dt, m->J, tag);
+    if ((e = spec_dir(g, s, 0, Fdx, Q, Yi, m, Dk, Fhx, th, tag, "flame_specViscousFlux_x")))
+        return e;
+    if ((e = spec_dir(g, s, 1, Fdy, Q, Yi, m, Dk, Fhy, th, tag, "flame_specViscousFlux_y")))
+        return e;
+    if ((e = spec_dir(g, s, 2, Fdz, Q, Yi, m, Dk, Fhz, th, tag, "flame_specViscousFlux_z")))
+        return e;
+    return flame_divSpecs(g, s, rhoi, Fxi, Fyi, Fzi, Fdx, Fdy, Fdz, dt, J, tag);
 }
 
 }  // extern "C"

@@ -25,6 +25,7 @@
 // Template parameters as in fused_stage.cu: NS species, QT storage of Q / transport, CT
 // arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
 
+#include <cstdint>
 #include <cstring>
 #include <type_traits>
 #include <utility>
@@ -48,6 +49,7 @@ struct Wpb {
 template <typename QT>
 struct Args {
     int nx, ny, nz, ng, tx, ty, tz, np, sy, sz;
+    int per;  // periodic axes (FlameGrid::periodic): ghost images are written on these only
     int stage;
     double dt, ca, cb;
     double *U, *Un;
@@ -515,18 +517,25 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
     }
     const double qv[7] = {rho, u, v, w, p, Tn, ei};
     const double tv[3] = {mu, lam, D};
-    // the cell and its periodic ghost images (new: the reference fills ghosts with case-specific
-    // kernels, boundary.jl:1-191)
+    // the cell and its ghost images along the periodic axes (new: the reference fills ghosts
+    // with case-specific kernels, boundary.jl:1-191, which the caller runs after the stage for
+    // the other axes)
     const int ng = A.ng;
     // up to two images per axis: an axis shorter than 2 NG has cells near both ends
     int ox[3] = {0, 0, 0}, oy[3] = {0, 0, 0}, oz[3] = {0, 0, 0};
     int nxo = 1, nyo = 1, nzo = 1;
-    if (gx < 2 * ng) ox[nxo++] = A.nx;
-    if (gx >= A.nx) ox[nxo++] = -A.nx;
-    if (gy < 2 * ng) oy[nyo++] = A.ny;
-    if (gy >= A.ny) oy[nyo++] = -A.ny;
-    if (gz < 2 * ng) oz[nzo++] = A.nz;
-    if (gz >= A.nz) oz[nzo++] = -A.nz;
+    if (A.per & 1) {
+        if (gx < 2 * ng) ox[nxo++] = A.nx;
+        if (gx >= A.nx) ox[nxo++] = -A.nx;
+    }
+    if (A.per & 2) {
+        if (gy < 2 * ng) oy[nyo++] = A.ny;
+        if (gy >= A.ny) oy[nyo++] = -A.ny;
+    }
+    if (A.per & 4) {
+        if (gz < 2 * ng) oz[nzo++] = A.nz;
+        if (gz >= A.nz) oz[nzo++] = -A.nz;
+    }
     for (int c = 0; c < nzo; ++c)
         for (int b = 0; b < nyo; ++b)
             for (int aa = 0; aa < nxo; ++aa) {
@@ -823,6 +832,7 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
     A.tx = g.nx + 2 * g.ng, A.ty = g.ny + 2 * g.ng, A.tz = g.nz + 2 * g.ng;
     A.np = A.tx * A.ty * A.tz;
     A.sy = A.tx, A.sz = A.tx * A.ty;
+    A.per = g.periodic & 7;
     A.stage = stage;
     A.dt = dt;
     A.ca = stage == 2 ? 0.25 : 2.0 / 3.0;
@@ -951,11 +961,16 @@ int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
                                                  scratch, split_finish != 0, split_species != 0);
 }
 
+// SIZE_MAX when the product does not fit in size_t (then no buffer can be large enough).
 extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
-    if (!g) return 0;
-    const size_t np = (size_t)(g->nx + 2 * g->ng) * (g->ny + 2 * g->ng) * (g->nz + 2 * g->ng);
+    if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ng < 0 || g->ns < 0) return 0;
     const size_t q = precision == 0 ? sizeof(double) : sizeof(float);
-    return np * (2 * (5 + g->ns) * sizeof(double) + (1 + g->ns) * q);
+    size_t bytes = 2 * (5 + (size_t)g->ns) * sizeof(double) + (1 + (size_t)g->ns) * q;
+    const size_t ext[3] = {(size_t)g->nx + 2 * (size_t)g->ng, (size_t)g->ny + 2 * (size_t)g->ng,
+                           (size_t)g->nz + 2 * (size_t)g->ng};
+    for (size_t e : ext)
+        if (__builtin_mul_overflow(bytes, e, &bytes)) return SIZE_MAX;
+    return bytes;
 }
 
 // ============================================================================= batches

@@ -84,6 +84,18 @@ class DeviceCase:
             self.U.copy_(torch.from_numpy(case.U()).to(dev))
         self.scratch = None
         self.seq = None
+        # the reference's own boundary conditions (not periodic): inflow / zero-gradient fills
+        # after every stage, as solver.jl:321-325 runs them after c2Prim
+        self.Yi = None
+        self.inflow = None
+        if case.periodic != 7:
+            if case.periodic != 0 or precision != 0:
+                raise abi.FlameError(5, "DeviceCase runs the reference's fills on grids periodic "
+                                        "on no axis, in FP64 (the fill kernels are FP64)")
+            from .cases import reference_inflow
+            self.inflow = case.inflow if case.inflow is not None else reference_inflow(ns)
+            self.Yi = torch.zeros((ns,) + shp, **f64)
+            self._fill(0)  # solver.jl:192-200: prim2c, then fillGhost and fillSpec
         self._transport()
         # tile: a configuration of flame_rk_stage_tiled, "auto" for the autotuner's choice, or
         # None for the pencil sweeps (configuration 3; with law 2 the library runs the pencil
@@ -94,6 +106,14 @@ class DeviceCase:
             self.set_tile(autotune.default().choose(self))
         if sequence_buffers:
             self._alloc_sequence()
+
+    def _fill(self, cur: int) -> None:
+        """The reference's ghost fills of state `cur` (boundary.jl:180-191): fillGhost on Q, U,
+        rho_i, then fillSpec on rho_i (one GPU: x-slab rank 0 of 1)."""
+        Q, r = self.Q[cur], self.rhoi[cur]
+        self._call("flame_fillGhost", _p(Q), _p(self.U), _p(r), _p(self.Yi), C.byref(self.thermo),
+                   C.byref(self.inflow), 0, 1)
+        self._call("flame_fillSpec", _p(r))
 
     def nonfinite_launch(self) -> torch.Tensor:
         """Queues flame_check_finite over U (solver.jl:388-391) and returns the device counter
@@ -130,8 +150,9 @@ class DeviceCase:
         them), optionally with another configuration."""
         c = DeviceCase.__new__(DeviceCase)
         for a in ("lib", "case", "device", "precision", "grid", "thermo", "transport", "dt",
-                  "metrics", "cmetrics", "cur", "poly", "metrics_lo"):
+                  "metrics", "cmetrics", "cur", "poly", "metrics_lo", "inflow"):
             setattr(c, a, getattr(self, a))
+        c.Yi = None if self.Yi is None else self.Yi.clone()
         c.Q = [q.clone() for q in self.Q]
         c.rhoi = [r.clone() for r in self.rhoi]
         c.T = [t.clone() for t in self.T]
@@ -194,19 +215,22 @@ class DeviceCase:
         self._call("flame_shockSensor", _p(w["phi"]), _p(Q))
         self._call("flame_specAdvance", _p(ri), _p(Q), _p(w["Yi"]), _p(w["Fpi"]), _p(w["Fmi"]),
                    _p(w["Fxi"]), _p(w["Fyi"]), _p(w["Fzi"]), _p(w["Fdx"]), _p(w["Fdy"]),
-                   _p(w["Fdz"]), g(self.cmetrics), dt, _p(w["phi"]), _p(w["D"]), _p(w["Fhx"]),
+                   _p(w["Fdz"]), *self.cmetrics.args(), dt, _p(w["phi"]), _p(w["D"]), _p(w["Fhx"]),
                    _p(w["Fhy"]), _p(w["Fhz"]), g(self.thermo), None)
         self._call("flame_flowAdvance", _p(self.U), _p(Q), _p(w["Fp"]), _p(w["Fm"]), _p(w["Fx"]),
                    _p(w["Fy"]), _p(w["Fz"]), _p(w["Fvx"]), _p(w["Fvy"]), _p(w["Fvz"]),
-                   g(self.cmetrics), dt, _p(w["phi"]), _p(w["lam"]), _p(w["mu"]), _p(w["Fhx"]),
+                   *self.cmetrics.args(), dt, _p(w["phi"]), _p(w["lam"]), _p(w["mu"]), _p(w["Fhx"]),
                    _p(w["Fhy"]), _p(w["Fhz"]), None)
         if stage in RK3:
             a, b = RK3[stage]
             self._call("flame_linComb", _p(self.U), _p(self.Un), 5, a, b, None)
             self._call("flame_linComb", _p(ri), _p(self.rhon), self.case.ns, a, b, None)
         self._call("flame_c2Prim", _p(self.U), _p(Q), _p(ri), g(self.thermo), None)
-        self._call("flame_fill_periodic", _p(Q), 7)
-        self._call("flame_fill_periodic", _p(ri), self.case.ns)
+        if self.inflow is not None:  # solver.jl:321-325
+            self._fill(self.cur)
+        else:
+            self._call("flame_fill_periodic", _p(Q), 7)
+            self._call("flame_fill_periodic", _p(ri), self.case.ns)
 
     def stage_fused(self, stage: int) -> None:
         """The same stage as one flame_rk_stage launch (ping-pong of Q and rho_i)."""
@@ -221,6 +245,10 @@ class DeviceCase:
                                            self.precision, self.tile)
         abi.check(self.lib, rc)
         self.cur = o
+        if self.inflow is not None:  # the ghosts of the result, then their transport
+            self._fill(o)
+            self._call("flame_transport_boundary", _p(self.Q[o]), _p(self.rhoi[o]), _p(self.T[o]),
+                       C.byref(self.thermo), C.byref(self.transport), self.precision)
 
     @property
     def launched_config(self) -> int:

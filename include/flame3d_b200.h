@@ -14,7 +14,10 @@
  *     which is the only value the fused entry points accept.
  *   - Every call is asynchronous on `stream` (NULL = legacy default stream) and returns
  *     FLAME_OK or an error code; flame_last_error() gives the message of the calling thread.
- *   - The library keeps no global mutable state besides a per-thread error string.
+ *   - Global state of the library: a per-thread error string; per device, flags recording that
+ *     a kernel's dynamic shared-memory limit has been raised (set once, never cleared); and,
+ *     used only by flame_rk_stage_noalloc, a library-held scratch array with its per-device
+ *     address cache (described at that entry point).  No call allocates device memory.
  *
  * The argument order after (grid, stream) is the argument order of the reference kernel each
  * entry point replaces, so a Julia `ccall` is a mechanical rewrite of the `@cuda` launch.
@@ -117,29 +120,50 @@ int flame_WENO_y(const FlameGrid *g, flame_stream_t stream, double *F, const dou
 int flame_WENO_z(const FlameGrid *g, flame_stream_t stream, double *F, const double *phi,
                  const double *Fp, const double *Fm, int NV, const int64_t *tag);
 
-/* viscous.jl:1-428  viscousFlux_x/y/z(Fv, Q, 9 metrics, J, λ, μ, Fh, tag); Fv is (faces, 4) */
+/* viscous.jl:1-428  viscousFlux_x/y/z(Fv, Q, dξdx, dξdy, dξdz, dηdx, dηdy, dηdz, dζdx, dζdy,
+ * dζdz, J, λ, μ, Fh, tag): the reference's argument list (viscous.jl:1, 144, 287), the nine
+ * J^-1-scaled metric cofactors and J as separate ghosted arrays.  Fv is (faces, 4). */
 int flame_viscousFlux_x(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *dxidx, const double *dxidy, const double *dxidz,
+                        const double *detadx, const double *detady, const double *detadz,
+                        const double *dzetadx, const double *dzetady, const double *dzetadz,
+                        const double *J, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag);
 int flame_viscousFlux_y(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *dxidx, const double *dxidy, const double *dxidz,
+                        const double *detadx, const double *detady, const double *detadz,
+                        const double *dzetadx, const double *dzetady, const double *dzetadz,
+                        const double *J, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag);
 int flame_viscousFlux_z(const FlameGrid *g, flame_stream_t stream, double *Fv, const double *Q,
-                        const FlameMetrics *m, const double *lambda, const double *mu,
+                        const double *dxidx, const double *dxidy, const double *dxidz,
+                        const double *detadx, const double *detady, const double *detadz,
+                        const double *dzetadx, const double *dzetady, const double *dzetadz,
+                        const double *J, const double *lambda, const double *mu,
                         const double *Fh, const int64_t *tag);
 
-/* viscous.jl:430-665  specViscousFlux_x/y/z(Fd, Q, Yi, 9 metrics, J, D, Fh, thermo, tag);
- * Fd is (faces, ns), Fh (faces, 3) is written. */
+/* viscous.jl:430-665  specViscousFlux_x/y/z(Fd, Q, Yi, dξdx, dξdy, dξdz, dηdx, dηdy, dηdz,
+ * dζdx, dζdy, dζdz, J, D, Fh, thermo, tag): the reference's argument list (viscous.jl:430, 509,
+ * 588).  Fd is (faces, ns), Fh (faces, 3) is written. */
 int flame_specViscousFlux_x(const FlameGrid *g, flame_stream_t stream, double *Fd,
-                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *Q, const double *Yi, const double *dxidx,
+                            const double *dxidy, const double *dxidz, const double *detadx,
+                            const double *detady, const double *detadz, const double *dzetadx,
+                            const double *dzetady, const double *dzetadz, const double *J,
                             const double *D, double *Fh, const FlameThermo *thermo,
                             const int64_t *tag);
 int flame_specViscousFlux_y(const FlameGrid *g, flame_stream_t stream, double *Fd,
-                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *Q, const double *Yi, const double *dxidx,
+                            const double *dxidy, const double *dxidz, const double *detadx,
+                            const double *detady, const double *detadz, const double *dzetadx,
+                            const double *dzetady, const double *dzetadz, const double *J,
                             const double *D, double *Fh, const FlameThermo *thermo,
                             const int64_t *tag);
 int flame_specViscousFlux_z(const FlameGrid *g, flame_stream_t stream, double *Fd,
-                            const double *Q, const double *Yi, const FlameMetrics *m,
+                            const double *Q, const double *Yi, const double *dxidx,
+                            const double *dxidy, const double *dxidz, const double *detadx,
+                            const double *detady, const double *detadz, const double *dzetadx,
+                            const double *dzetady, const double *dzetadz, const double *J,
                             const double *D, double *Fh, const FlameThermo *thermo,
                             const int64_t *tag);
 
@@ -270,28 +294,42 @@ int flame_check_finite(const FlameGrid *g, flame_stream_t stream, const double *
 int flame_cfl_max(const FlameGrid *g, flame_stream_t stream, const double *Q,
                   const FlameMetrics *m, double *out);
 
-/* solver.jl:22-38  flowAdvance(…): fluxSplit+WENO per direction, viscousFlux ×3, div.
- * Fp/Fm are ghosted (…,5) scratch; Fx/Fy/Fz face (…,5); Fv_* face (…,4); Fh* face (…,3). */
+/* solver.jl:22-38  flowAdvance(U, Q, Fp, Fm, Fx, Fy, Fz, Fv_x, Fv_y, Fv_z, dξdx, dξdy, dξdz,
+ * dηdx, dηdy, dηdz, dζdx, dζdy, dζdz, J, dt, ϕ, λ, μ, Fhx, Fhy, Fhz, tag): fluxSplit+WENO per
+ * direction, viscousFlux ×3, div.  Fp/Fm are ghosted (…,5) scratch; Fx/Fy/Fz face (…,5);
+ * Fv_* face (…,4); Fh* face (…,3). */
 int flame_flowAdvance(const FlameGrid *g, flame_stream_t stream, double *U, const double *Q,
                       double *Fp, double *Fm, double *Fx, double *Fy, double *Fz, double *Fv_x,
-                      double *Fv_y, double *Fv_z, const FlameMetrics *m, double dt,
-                      const double *phi, const double *lambda, const double *mu,
-                      const double *Fhx, const double *Fhy, const double *Fhz,
-                      const int64_t *tag);
+                      double *Fv_y, double *Fv_z, const double *dxidx, const double *dxidy,
+                      const double *dxidz, const double *detadx, const double *detady,
+                      const double *detadz, const double *dzetadx, const double *dzetady,
+                      const double *dzetadz, const double *J, double dt, const double *phi,
+                      const double *lambda, const double *mu, const double *Fhx,
+                      const double *Fhy, const double *Fhz, const int64_t *tag);
 
-/* solver.jl:40-56  specAdvance(…): split+WENO per direction, specViscousFlux ×3, divSpecs. */
+/* solver.jl:40-56  specAdvance(ρi, Q, Yi, Fp_i, Fm_i, Fx_i, Fy_i, Fz_i, Fd_x, Fd_y, Fd_z, dξdx,
+ * dξdy, dξdz, dηdx, dηdy, dηdz, dζdx, dζdy, dζdz, J, dt, ϕ, D, Fhx, Fhy, Fhz, thermo, tag):
+ * split+WENO per direction, specViscousFlux ×3, divSpecs. */
 int flame_specAdvance(const FlameGrid *g, flame_stream_t stream, double *rhoi, const double *Q,
                       const double *Yi, double *Fp_i, double *Fm_i, double *Fx_i, double *Fy_i,
                       double *Fz_i, double *Fd_x, double *Fd_y, double *Fd_z,
-                      const FlameMetrics *m, double dt, const double *phi, const double *D,
+                      const double *dxidx, const double *dxidy, const double *dxidz,
+                      const double *detadx, const double *detady, const double *detadz,
+                      const double *dzetadx, const double *dzetady, const double *dzetadz,
+                      const double *J, double dt, const double *phi, const double *D,
                       double *Fhx, double *Fhy, double *Fhz, const FlameThermo *thermo,
                       const int64_t *tag);
 
 /* ---------------------------------------------------------------------------------------
- * Fused path: one launch per RK3 stage (solver.jl:297-326 for periodic grids, IBM off).
+ * Fused path: one RK3 stage in one to seven launches (solver.jl:297-326, IBM off).
  * Reads Q_in / rhoi_in / trans_in (ghosts filled), writes U in place and Q_out / rhoi_out /
- * trans_out including their periodic ghost images, so the caller swaps every in/out pair after
- * each stage.  Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
+ * trans_out on the interior cells and, along every periodic axis (FlameGrid::periodic), their
+ * ghost images, so the caller swaps every in/out pair after each stage.  On an axis that is not
+ * periodic the stage writes interior cells only, and the caller fills the ghosts of the result
+ * as the reference does after c2Prim (solver.jl:321-325): flame_fillGhost on (Q_out, U,
+ * rhoi_out), flame_fillSpec on rhoi_out, then flame_transport_boundary on (Q_out, rhoi_out,
+ * trans_out) for the points the fills changed (FP64 storage, precision 0: the fills are FP64).
+ * Stage 1 also writes Un = U and rhon = rhoi (solver.jl:299-302).
  * trans_* hold the transport of the state, (…, 3) = μ, λ, D, as computed by flame_transport;
  * with law 2 (mixture-averaged, per-species D_k) they are (…, 2 + ns) = μ, λ, D_0 .. D_{ns-1}.
  * The stage computes the next one in its epilogue, so the law is evaluated once per cell.
@@ -366,6 +404,15 @@ int flame_rk_stage_noalloc(const FlameGrid *g, flame_stream_t stream, int stage,
 int flame_transport(const FlameGrid *g, flame_stream_t stream, const void *Q, const double *rhoi,
                     void *trans, const FlameThermo *thermo, const FlameTransport *transport,
                     int precision);
+
+/* flame_transport restricted to the points a ghost fill can change on a grid that is not
+ * periodic on every axis: on each non-periodic axis the ghost layers and the first and last
+ * interior planes (the planes the reference's fill_x / fill_y / fill_z and fill_y_s / fill_z_s
+ * overwrite, boundary.jl:1-176).  Nothing to do on a fully periodic grid.  New: the reference
+ * recomputes the whole mixture every stage (solver.jl:304). */
+int flame_transport_boundary(const FlameGrid *g, flame_stream_t stream, const void *Q,
+                             const double *rhoi, void *trans, const FlameThermo *thermo,
+                             const FlameTransport *transport, int precision);
 
 /* ---------------------------------------------------------------------------------------
  * Batches (no reference counterpart): many independent periodic cases, each with its own

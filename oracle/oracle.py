@@ -130,11 +130,32 @@ class OracleCase:
         self.Un = np.empty_like(self.U)
         self.rhon = np.empty_like(self.rhoi)
         self.dt = case.dt
+        # not periodic: the reference's fills after prim2c and after every stage
+        # (solver.jl:192-200, 321-325); the stage's periodic fill then does nothing
+        self.inflow = None
+        if case.periodic != 7:
+            self.inflow = getattr(case, "inflow", None)
+            self.Yi = np.zeros_like(self.rhoi)
+            self.fill()
+
+    def fill(self) -> None:
+        """fillGhost (fill_x, fill_y, fill_z) and fillSpec (fill_y_s, fill_z_s),
+        boundary.jl:180-191, on rank 0 of 1."""
+        g, th, P = C.byref(self.grid), C.byref(self.th), ptr
+        self.lib.oracle_fill_x(g, P(self.Q), P(self.U), P(self.rhoi), P(self.Yi), th,
+                               C.byref(self.inflow), 0, 1)
+        self.lib.oracle_fill_y(g, P(self.Q), P(self.U), None)
+        self.lib.oracle_fill_z(g, P(self.Q), P(self.U), P(self.rhoi), P(self.Yi), th,
+                               C.byref(self.inflow))
+        self.lib.oracle_fill_y(g, None, None, P(self.rhoi))
+        self.lib.oracle_fill_z_s(g, P(self.rhoi))
 
     def stage(self, s: int) -> None:
         self.lib.oracle_rk_stage_seq(C.byref(self.grid), s, self.dt, ptr(self.U), ptr(self.Un),
                                      ptr(self.Q), ptr(self.rhoi), ptr(self.rhon),
                                      C.byref(self.cm), C.byref(self.th), C.byref(self.tr))
+        if self.inflow is not None:
+            self.fill()
 
     def step(self) -> None:
         for s in (1, 2, 3):

@@ -59,14 +59,14 @@ def test_argument_errors_need_no_gpu(f3d, lib):
     g = f3d.FlameGrid(8, 8, 8, 4, 0, 7)
     assert lib.flame_split(C.byref(g), None, 1, 1, 1, 1, 1, 1, 1, None) == 1
     assert "ns=0" in f3d.abi.last_error(lib)
-    # the fused stage refuses non-periodic grids and unknown precisions before launching
+    # the fused stage refuses unknown precisions, stages and aliased buffers before launching
     g = f3d.FlameGrid(8, 8, 8, 4, 1, 3)
     b = f3d.FlameStageBuffers(1, 2, 3, 4, 5, 6, 7, 8, 9)
     m = f3d.FlameMetrics(*([1] * 10))
     th, tr = f3d.FlameThermo(), f3d.FlameTransport()
     rc = lib.flame_rk_stage(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m), C.byref(th),
-                            C.byref(tr), 0)
-    assert rc == 5 and "periodic" in f3d.abi.last_error(lib)
+                            C.byref(tr), 2)
+    assert rc == 1 and "precision" in f3d.abi.last_error(lib)
     g = f3d.FlameGrid(8, 8, 8, 4, 1, 7)
     rc = lib.flame_rk_stage(C.byref(g), None, 4, 1e-3, C.byref(b), C.byref(m), C.byref(th),
                             C.byref(tr), 0)
@@ -82,3 +82,39 @@ def test_python_raises_flame_error(f3d, lib):
     with pytest.raises(f3d.FlameError) as e:
         f3d.abi.check(lib, lib.flame_prim2c(None, None, 1, 1))
     assert e.value.code == 1
+
+
+def test_signature_arity_matches_header(f3d):
+    """Every declaration's parameter count equals the ctypes table's, so a call made from Python
+    (or a Julia ccall written from the header) passes the arguments the library reads."""
+    import re
+    text = re.sub(r"/\*.*?\*/", "", f3d.abi.HEADER.read_text(), flags=re.S)
+    decls = re.findall(r"\b(?:int|size_t)\s+(flame_\w+)\s*\(([^)]*)\)\s*;", text)
+    assert decls
+    for name, params in decls:
+        n = 0 if params.strip() in ("", "void") else params.count(",") + 1
+        assert n == len(f3d.abi.SIGNATURES[name]), (name, n, len(f3d.abi.SIGNATURES[name]))
+
+
+def test_viscous_entry_points_take_the_reference_argument_list(f3d):
+    """viscousFlux_x(Fv_x, Q, dξdx, dξdy, dξdz, dηdx, dηdy, dηdz, dζdx, dζdy, dζdz, J, λ, μ, Fh,
+    tag) (viscous.jl:1) and specViscousFlux_x(Fd, Q, Yi, 9 metrics, J, D, Fh, thermo, tag)
+    (viscous.jl:430): the metrics are ten separate arrays after (grid, stream)."""
+    import re
+    text = re.sub(r"/\*.*?\*/", "", f3d.abi.HEADER.read_text(), flags=re.S)
+    metric = ["dxidx", "dxidy", "dxidz", "detadx", "detady", "detadz", "dzetadx", "dzetady",
+              "dzetadz", "J"]
+    want = {"flame_viscousFlux": ["Fv", "Q", *metric, "lambda", "mu", "Fh", "tag"],
+            "flame_specViscousFlux": ["Fd", "Q", "Yi", *metric, "D", "Fh", "thermo", "tag"],
+            "flame_flowAdvance": ["U", "Q", "Fp", "Fm", "Fx", "Fy", "Fz", "Fv_x", "Fv_y", "Fv_z",
+                                  *metric, "dt", "phi", "lambda", "mu", "Fhx", "Fhy", "Fhz",
+                                  "tag"],
+            "flame_specAdvance": ["rhoi", "Q", "Yi", "Fp_i", "Fm_i", "Fx_i", "Fy_i", "Fz_i",
+                                  "Fd_x", "Fd_y", "Fd_z", *metric, "dt", "phi", "D", "Fhx",
+                                  "Fhy", "Fhz", "thermo", "tag"]}
+    for stem, names in want.items():
+        sfx = ["_x", "_y", "_z"] if "Flux" in stem else [""]
+        for s in sfx:
+            m = re.search(rf"\b{stem}{s}\s*\(([^)]*)\)", text)
+            got = [re.findall(r"(\w+)\s*$", a.strip())[0] for a in m.group(1).split(",")][2:]
+            assert got == names, (stem + s, got)

@@ -163,15 +163,16 @@ def test_viscous_and_species_diffusion(env, d):
                                     C.byref(env.cm_host), P(D), P(Fh_h), C.byref(env.th), None)
     Fd_d, Fh_d = _t(np.zeros((ns,) + fs)), _t(np.zeros((3,) + fs))
     sfx = "xyz"[d]
+    # the reference's argument list: the nine metric cofactors and J one by one
     env.gcall(f"flame_specViscousFlux_{sfx}", P(Fd_d), P(_t(env.Q)), P(_t(Yi)),
-              C.byref(env.cm_dev), P(_t(D)), P(Fh_d), C.byref(env.th), None)
+              *env.cm_dev.args(), P(_t(D)), P(Fh_d), C.byref(env.th), None)
     exact(_np(Fd_d), Fd_h)
     exact(_np(Fh_d), Fh_h)
     Fv_h = np.zeros((4,) + fs)
     env.olib.oracle_viscousFlux(C.byref(env.g), d, P(Fv_h), P(env.Q), C.byref(env.cm_host),
                                 P(lam), P(mu), P(Fh_h), None)
     Fv_d = _t(np.zeros((4,) + fs))
-    env.gcall(f"flame_viscousFlux_{sfx}", P(Fv_d), P(_t(env.Q)), C.byref(env.cm_dev),
+    env.gcall(f"flame_viscousFlux_{sfx}", P(Fv_d), P(_t(env.Q)), *env.cm_dev.args(),
               P(_t(lam)), P(_t(mu)), P(Fh_d), None)
     exact(_np(Fv_d), Fv_h)
 
