@@ -12,7 +12,8 @@
 //   * at most FLAME_NOALLOC_SCRATCH_BYTES of scratch, i.e. grids whose
 //     flame_stage_scratch_bytes() fits; larger grids are rejected with FLAME_EINVAL;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current, so it should be made before any stream capture;
+//     that device current, so it should be made before any stream capture; the address is cached
+//     for the life of the process, so cudaDeviceReset between calls is not supported;
 //   * every call on a device shares the one array, so calls that overlap on the GPU (different
 //     streams, or different host threads) race and must be serialised by the caller;
 //   * nothing in the array has to start at zero: each stage writes the accumulator and the

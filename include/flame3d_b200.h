@@ -389,9 +389,11 @@ size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision);
  * on every device it is loaded on until the process exits; b->scratch is ignored.  Grids whose
  * flame_stage_scratch_bytes() exceeds it are rejected with FLAME_EINVAL (FP64, ns = 1: up to
  * about 600 thousand ghosted points).  The first call on a device looks up the array's address
- * with that device current, so make it before any stream capture.  All calls on a device share
- * the array: calls that overlap on the GPU race and must be serialised by the caller.  Nothing
- * in the array has to start at zero; allocates nothing. */
+ * with that device current, so make it before any stream capture; the address is then cached
+ * for the life of the process, so cudaDeviceReset between calls is not supported (the array
+ * may come back at another address).  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  Nothing in the array has to
+ * start at zero; allocates nothing. */
 #define FLAME_NOALLOC_SCRATCH_BYTES (64u << 20)
 int flame_rk_stage_noalloc(const FlameGrid *g, flame_stream_t stream, int stage, double dt,
                            const FlameStageBuffers *b, const FlameMetrics *m,

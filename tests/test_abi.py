@@ -118,3 +118,19 @@ def test_viscous_entry_points_take_the_reference_argument_list(f3d):
             m = re.search(rf"\b{stem}{s}\s*\(([^)]*)\)", text)
             got = [re.findall(r"(\w+)\s*$", a.strip())[0] for a in m.group(1).split(",")][2:]
             assert got == names, (stem + s, got)
+
+
+def test_size_queries_do_not_wrap(f3d, lib):
+    """flame_stage_scratch_bytes saturates instead of wrapping, and the stage's size check
+    rejects extents whose point count would overflow, before any CUDA call."""
+    big = f3d.FlameGrid(2**31 - 9, 2**31 - 9, 2**31 - 9, 4, 1, 7)
+    assert lib.flame_stage_scratch_bytes(C.byref(big), 0) == 2**64 - 1
+    g = f3d.FlameGrid(64, 32, 32, 4, 1, 7)
+    assert lib.flame_stage_scratch_bytes(C.byref(g), 0) == 72 * 40 * 40 * (2 * 6 * 8 + 2 * 8)
+    b = f3d.FlameStageBuffers(1, 2, 3, 4, 5, 6, 7, 8, 9)
+    m = f3d.FlameMetrics(*([1] * 10))
+    for ext in ((1 << 21,) * 3, (2**31 - 9,) * 3, (100000, 100000, 4)):
+        g = f3d.FlameGrid(*ext, 4, 1, 7)
+        rc = lib.flame_rk_stage(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m),
+                                C.byref(f3d.FlameThermo()), C.byref(f3d.FlameTransport()), 0)
+        assert rc == 1 and "2^31" in f3d.abi.last_error(lib), ext

@@ -36,11 +36,19 @@ def _noalloc_stage(f3d, dc, stage):
     dc.cur = o
 
 
+def _case(f3d, law):
+    case = f3d.random_curvilinear(n=12, ns=2 if law == 1 else 3, seed=7)
+    if law == 2:  # the mixture-averaged law: the stage runs configuration 6's launches
+        case.transport = f3d.cases.mixture_averaged_transport(case.thermo, seed=3)
+    return case
+
+
+@pytest.mark.parametrize("law", [1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_noalloc_matches_caller_scratch_two_calls(f3d, cuda_ok, precision):
+def test_noalloc_matches_caller_scratch_two_calls(f3d, cuda_ok, precision, law):
     import torch
     S = f3d.solver_module()
-    case = f3d.random_curvilinear(n=12, ns=2, seed=7)
+    case = _case(f3d, law)
     ref = S.DeviceCase(case, precision=precision, tile=3)
     new = S.DeviceCase(case, precision=precision, tile=3)
     for stage in (1, 2):
@@ -58,9 +66,13 @@ def test_noalloc_matches_caller_scratch_two_calls(f3d, cuda_ok, precision):
         assert np.isfinite(Un).all()
 
 
-def test_noalloc_rejects_grids_beyond_its_scratch(f3d, cuda_ok):
+@pytest.mark.parametrize("ext", [(512, 512, 256), (1 << 21, 1 << 21, 1 << 21),
+                                 (2**31 - 9, 2**31 - 9, 2**31 - 9)])
+def test_noalloc_rejects_grids_beyond_its_scratch(f3d, cuda_ok, ext):
+    """Too large for the library's array, including extents whose scratch size would wrap a
+    64-bit product: rejected before any launch."""
     lib = f3d.load_library()
-    g = f3d.FlameGrid(512, 512, 256, 4, 1, 7)
+    g = f3d.FlameGrid(*ext, 4, 1, 7)
     assert lib.flame_stage_scratch_bytes(C.byref(g), 0) > (64 << 20)
     b = f3d.FlameStageBuffers(*([1] * 10))
     m = f3d.FlameMetrics(*([1] * 10))
