@@ -15,6 +15,19 @@ one-launch-per-stage kernel.  A "step" is one SSP-RK3 step (three stages).
   cpu_baseline  the oracle (C++ FP64 restatement, OpenMP over all host cores) on a bounded
          sample of the same workload
 
+  fp64 (in roofline)  the same stage against the measured FP64 FMA peak (libflame3d_probe.so):
+         FP64 FLOPs per cell-stage from the ncu instruction counts in profiles/ncu_fp64.json
+
+On one GPU the default (jet) run also measures, in the same JSON line: the reference's own
+launch sequence of 1:1 kernels on the jet (`launch_sequence`), the mixed-precision stage on the
+jet with its error against the FP64 stage after a bounded number of steps (`mixed`), and the
+batched mixed-precision ensemble of 64 cases against the plain FP64 paths one case at a time,
+with step p50/p99 and a bounded error check (`ensemble64`): the "batched mixed-prec" half of
+the metric.  `--no-extras` skips them.
+
+`--gpus N` without torchrun launches itself under torch.distributed.run with N ranks (one
+process per GPU, replicas; rendezvous on 127.0.0.1).
+
 `--impl reference` times the reference path's CPU implementation instead (the oracle port:
 the reference's RHS exists only as Julia CUDA.jl kernels and Julia is not installed).
 """
@@ -37,6 +50,7 @@ UNIT = "Mcell-stage/s"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 E2E_LANES = 3  # cases / streams the end-to-end calls rotate over
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
+FP64_COUNTS = ROOT / "profiles" / "ncu_fp64.json"
 
 
 def _package():
@@ -172,38 +186,73 @@ def cpu_sample(f3d, workload: str, stages: int):
 
 
 def run_reference(args, f3d):
+    """The reference path's CPU implementation (the oracle port, all host threads) on a bounded
+    sample of the workload: each step is one full RK3 step (three stages) of a 1/8 slab.  Under
+    N ranks only rank 0 works; the ranks meet in a gloo process group so that every rank takes
+    the same collective steps, and rank 0 prints the line with the N it ran under."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle
-    lib = oracle.load()
-    if WORKLOADS[args.workload]["kind"] not in ("jet", "tgv", "mixing"):
-        args.workload = "jet256x128x128"  # case-set workloads: the reference RHS on the jet
-    w = WORKLOADS[args.workload]
-    nz = 16 if w["kind"] == "jet" else None
-    case = make_case(f3d, args.workload, nz_override=nz) if nz else make_case(f3d, args.workload)
-    oc = oracle.OracleCase(case)
-    for s in range(args.warmup):
-        oc.stage(1 + s % 3)
-    t0 = time.perf_counter()
-    for s in range(args.steps):
-        oc.stage(1 + s % 3)
-    dt = time.perf_counter() - t0
-    value = case.cells * args.steps / dt / 1e6
-    sample = (f"each step = 1 RK3 stage of the oracle (C++ FP64 restatement of the reference "
-              f"RHS) on a {case.nx}x{case.ny}x{case.nz} slab of the same workload")
-    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": args.workload, "sample_cells": case.cells},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": lib.oracle_num_threads(),
-                            "kind": "port", "sample": sample},
-           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                   "d2h_bytes_per_step": 0}}
-    print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    line = None
+    if rank == 0:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        lib = oracle.load()
+        if WORKLOADS[args.workload]["kind"] not in ("jet", "tgv", "mixing"):
+            args.workload = "jet256x128x128"  # case-set workloads: the reference RHS on the jet
+        w = WORKLOADS[args.workload]
+        nz = 16 if w["kind"] == "jet" else None
+        case = make_case(f3d, args.workload, nz_override=nz) if nz else make_case(f3d, args.workload)
+        oc = oracle.OracleCase(case)
+        for _ in range(args.warmup):
+            oc.step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            oc.step()
+        dt = time.perf_counter() - t0
+        value = case.cells * 3 * args.steps / dt / 1e6
+        sample = (f"each step = one RK3 step (3 stages) of the oracle (C++ FP64 restatement of "
+                  f"the reference RHS) on a {case.nx}x{case.ny}x{case.nz} slab of the workload")
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "sample_cells": case.cells,
+                           "step": "one RK3 step of the sample slab"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": lib.oracle_num_threads(),
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
     return 0
+
+
+def _free_port() -> int:
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def relaunch_cmd(n: int, argv: list[str], port: int | None = None) -> list[str]:
+    """The torch.distributed.run command that runs this script with n ranks on this node."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={n}", "--master-addr=127.0.0.1",
+            f"--master-port={port or _free_port()}", str(Path(__file__).resolve()), *argv]
+
+
+def relaunch(n: int, argv: list[str]) -> int:
+    """--gpus N > 1 without torchrun: run N ranks of this script (one process per GPU) and
+    return the launcher's status; rank 0's JSON line reaches stdout."""
+    return subprocess.run(relaunch_cmd(n, argv)).returncode
 
 
 # ------------------------------------------------------------------------------ ensemble
@@ -212,20 +261,21 @@ def _pct(xs, q):
     return xs[min(len(xs) - 1, int(round(q / 100 * (len(xs) - 1))))]
 
 
-def run_ensemble(args, f3d) -> int:
-    """64 independent periodic cases (sizes 32^3-128^3, 1-9 species): the batched mixed-precision
-    path (one graph replay per RK3 step for all cases) against the plain FP64 paths advancing one
-    case at a time (FIFO): the fused pencil stage and the reference launch sequence of 1:1
-    kernels.  Device-timed with CUDA events."""
+def ensemble_record(f3d, dev, k: int, warm: int = 3, check_steps: int = 20) -> dict:
+    """64 independent periodic cases (sizes 32^3-128^3, 1-9 species): the batched
+    mixed-precision path (one graph replay per RK3 step for all cases; persistent kernels as
+    the other mode) against the plain FP64 paths advancing one case at a time (FIFO): the fused
+    pencil stage and the reference launch sequence of 1:1 kernels.  Device-timed with CUDA
+    events.  Error check: four cases (the smallest and largest, fewest and most species)
+    advanced `check_steps` RK3 steps in a mixed-precision graph batch against the plain FP64
+    stage from the same state, relative L2 of rho, rho*u, rho*E."""
     import torch
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
     S, B = f3d.solver_module(), f3d.batch_module()
     cases = f3d.cases.ensemble(64, seed=4)
     cells = sum(c.cells for c in cases)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def fifo(precision, fused, k):
+    def fifo(precision, fused, n):
         tot = 0.0
         for c in cases:
             dc = S.DeviceCase(c, device=dev, precision=precision, tile="auto" if fused else 3,
@@ -233,26 +283,25 @@ def run_ensemble(args, f3d) -> int:
             dc.step(fused)
             torch.cuda.synchronize(dev)
             e0.record()
-            for _ in range(k):
+            for _ in range(n):
                 dc.step(fused)
             e1.record()
             torch.cuda.synchronize(dev)
             tot += e0.elapsed_time(e1)
             del dc
             torch.cuda.empty_cache()
-        return cells * 3 * k / (tot / 1e3) / 1e6, tot / k
+        return cells * 3 * n / (tot / 1e3) / 1e6, tot / n
 
     plain, plain_ms = fifo(0, True, 3)
     seq, seq_ms = fifo(0, False, 1)
     pencil = [S.DeviceCase(c, device=dev, precision=1, tile=3) for c in cases]
     tuned = [S.DeviceCase(c, device=dev, precision=1, tile="auto") for c in cases]
-    k = max(args.steps // 10, 10)
     modes = {}
     for mode, dcs, nst in (("graph", tuned, 16), ("graph_s32", tuned, 32),
                            ("graph_pencil", pencil, 16), ("persistent", pencil, 16)):
         batch = B.Batch(dcs, device=dev, mode=mode.split("_")[0], streams=nst)
         batch.capture()
-        for _ in range(max(args.warmup, 3)):
+        for _ in range(warm):
             batch.step()
         torch.cuda.synchronize(dev)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
@@ -267,26 +316,64 @@ def run_ensemble(args, f3d) -> int:
         batch.close()
     best = max(modes, key=lambda m: modes[m][0])
     value, ms, per_step = modes[best]
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": k,
-           "warmup": max(args.warmup, 3), "ms_per_step": ms / k, "higher_is_better": True,
+    launches = (3 * sum(d.launches_per_stage() for d in tuned) if best in ("graph", "graph_s32")
+                else 3 * sum(d.launches_per_stage() for d in pencil) if best == "graph_pencil"
+                else 3 * 4 * len({c.ns for c in cases}))
+    del pencil, tuned
+    torch.cuda.empty_cache()
+    # bounded error check
+    pick = sorted(range(len(cases)), key=lambda i: (cases[i].cells, cases[i].ns))
+    pick = sorted({pick[0], pick[-1], min(range(len(cases)), key=lambda i: cases[i].ns),
+                   max(range(len(cases)), key=lambda i: cases[i].ns)})
+    mixed = [S.DeviceCase(cases[i], device=dev, precision=1, tile="auto") for i in pick]
+    batch = B.Batch(mixed, device=dev, mode="graph")
+    for _ in range(check_steps):
+        batch.step()
+    batch.close()
+    errs = {}
+    for dc, i in zip(mixed, pick):
+        ref = S.DeviceCase(cases[i], device=dev, precision=0, tile="auto")
+        for _ in range(check_steps):
+            ref.step()
+        errs[cases[i].name] = _conserved_errors(dc.conserved(), ref.conserved(),
+                                                lambda a: a[..., 4:-4, 4:-4, 4:-4])
+        del ref
+    del mixed
+    torch.cuda.empty_cache()
+    worst = {f: max(e[f] for e in errs.values()) for f in ("rho", "rhou", "rhoE")}
+    return {"value": value, "unit": UNIT, "steps": k, "warmup": warm, "ms_per_step": ms / k,
+            "dtype": "f32/f64", "cases": len(cases), "cells": cells,
+            "path": f"batched stages ({best} mode), mixed precision, CUDA graph per step",
+            "modes": {m: v[0] for m, v in modes.items()},
+            "launches_per_step": launches,
+            "step_latency_ms": {"p50": _pct(per_step, 50), "p99": _pct(per_step, 99)},
+            "plain_fp64_fused_fifo": {"value": plain, "unit": UNIT,
+                                      "ms_per_step_all_cases": plain_ms},
+            "plain_fp64_launch_sequence_fifo": {"value": seq, "unit": UNIT,
+                                                "ms_per_step_all_cases": seq_ms},
+            "speedup_vs_plain_fp64_fused": value / plain,
+            "speedup_vs_launch_sequence": value / seq,
+            "error_check": {"steps": check_steps, "cases": errs, "max_rel_l2": worst,
+                            "against": "plain FP64 fused stage from the same state"}}
+
+
+def run_ensemble(args, f3d) -> int:
+    """--workload ensemble64: the ensemble record as the JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    r = ensemble_record(f3d, dev, max(args.steps // 10, 10), max(args.warmup, 3))
+    out = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["steps"],
+           "warmup": r["warmup"], "ms_per_step": r["ms_per_step"], "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
            "data": "synthetic (seeded Taylor-Green ensemble with Fourier perturbations)",
-           "config": {"workload": "ensemble64", "cases": len(cases), "cells": cells,
-                      "path": f"batched stages ({best} mode), mixed precision, CUDA graph per step",
-                      "modes": {m: v[0] for m, v in modes.items()},
-                      "tuned_configs": {str(t): sum(d.tile == t for d in tuned)
-                                        for t in sorted({d.tile for d in tuned})},
-                      "launches_per_step": (3 * sum(d.launches_per_stage() for d in tuned)
-                                            if best in ("graph", "graph_s32") else
-                                            3 * sum(d.launches_per_stage() for d in pencil)
-                                            if best == "graph_pencil" else
-                                            3 * 4 * len({c.ns for c in cases}))},
-           "step_latency_ms": {"p50": _pct(per_step, 50), "p99": _pct(per_step, 99)},
-           "plain_fp64_fused_fifo": {"value": plain, "unit": UNIT, "ms_per_step_all_cases": plain_ms},
-           "plain_fp64_launch_sequence_fifo": {"value": seq, "unit": UNIT,
-                                               "ms_per_step_all_cases": seq_ms},
-           "speedup_vs_plain_fp64_fused": value / plain,
-           "speedup_vs_launch_sequence": value / seq}
+           "config": {"workload": "ensemble64", "cases": r["cases"], "cells": r["cells"],
+                      "path": r["path"], "modes": r["modes"],
+                      "launches_per_step": r["launches_per_step"]},
+           **{key: r[key] for key in ("step_latency_ms", "plain_fp64_fused_fifo",
+                                     "plain_fp64_launch_sequence_fifo",
+                                     "speedup_vs_plain_fp64_fused", "speedup_vs_launch_sequence",
+                                     "error_check")}}
     print(json.dumps(out), flush=True)
     return 0
 
@@ -437,6 +524,88 @@ def run_serve(args, f3d) -> int:
     return 0
 
 
+# ------------------------------------------------------------------------------ FP64 roof
+def fp64_peak_tflops(f3d, dev) -> float | None:
+    """Measured FP64 FMA throughput of this GPU in TFLOP/s: the project's probe kernel
+    (csrc/probe/fp64_peak.cu, eight independent FMA chains per thread, 8 blocks of 256 threads
+    per SM), CUDA events over five launches after two warm-ups."""
+    import ctypes as C
+    import importlib
+
+    import torch
+    try:
+        path = importlib.import_module(f3d.__name__ + ".build").build_probe()
+    except (RuntimeError, OSError):
+        return None
+    lib = C.CDLL(str(path))
+    fn = lib.flame_probe_fp64_fma
+    fn.restype, fn.argtypes = C.c_double, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    blocks = 8 * torch.cuda.get_device_properties(dev).multi_processor_count
+    out = torch.empty(blocks * 256, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev)
+    for _ in range(2):
+        fn(blocks, 4000, out.data_ptr(), s.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    flops = sum(fn(blocks, 10000, out.data_ptr(), s.cuda_stream) for _ in range(5))
+    e1.record(s)
+    torch.cuda.synchronize(dev)
+    return flops / (e0.elapsed_time(e1) / 1e3) / 1e12 if flops > 0 else None
+
+
+# ------------------------------------------------------------------------------ extras
+def _device_rate(dc, steps: int, warm: int = 1, fused: bool = True):
+    """Mcell-stage/s of `steps` RK3 steps of one DeviceCase, CUDA events on its stream."""
+    import torch
+    for _ in range(warm):
+        dc.step(fused)
+    st = torch.cuda.current_stream(dc.device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dc.device)
+    e0.record(st)
+    for _ in range(steps):
+        dc.step(fused)
+    e1.record(st)
+    torch.cuda.synchronize(dc.device)
+    ms = e0.elapsed_time(e1)
+    return dc.case.cells * 3 * steps / (ms / 1e3) / 1e6, ms / steps
+
+
+def launch_sequence_record(f3d, case, dev, steps: int = 2) -> dict:
+    """The reference's own kernel structure on the same GPU: solver.jl:298-326 as ~30 launches
+    of the 1:1 entry points per stage (plain FP64), the literal drop-in."""
+    import torch
+    dc = f3d.solver_module().DeviceCase(case, device=dev, sequence_buffers=True)
+    rate, ms = _device_rate(dc, steps, fused=False)
+    del dc
+    torch.cuda.empty_cache()
+    return {"value": rate, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "path": "1:1 entry points, the reference's launch sequence (solver.jl:298-326)"}
+
+
+def mixed_record(f3d, case, dev, steps: int) -> dict:
+    """Mixed precision on the same workload: its device-timed rate, and after `steps` RK3 steps
+    from the same initial state its relative L2 error in rho, rho*u, rho*E against the plain
+    FP64 stage (itself within 1e-12 of the oracle per stage in the parity tests)."""
+    import numpy as np
+    import torch
+    S = f3d.solver_module()
+    mixed = S.DeviceCase(case, device=dev, precision=1, tile="auto")
+    fp64 = S.DeviceCase(case, device=dev, precision=0, tile="auto")
+    for _ in range(steps):
+        mixed.step()
+        fp64.step()
+    U, Uref = mixed.conserved(), fp64.conserved()
+    err = _conserved_errors(U, Uref, lambda a: a[..., 4:-4, 4:-4, 4:-4])
+    rate, ms = _device_rate(mixed, 10)
+    out = {"value": rate, "unit": UNIT, "ms_per_step": ms, "stage_config": mixed.launched_config,
+           "error_vs_fp64_after_steps": steps, "rel_l2": err,
+           "finite": bool(np.isfinite(U).all())}
+    del mixed, fp64
+    torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------------------------ replicas
 def max_over_ranks(ms: float, device=None) -> float:
     """The slowest rank's time: N replicas are done when the last one is (all_reduce MAX; on
@@ -478,8 +647,14 @@ def main() -> int:
                     help="serve: also time the 1:1 launch-sequence FIFO (about a minute more)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="precision: RK3 steps before the errors are measured")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="jet workload: skip the launch-sequence, mixed and ensemble records")
+    ap.add_argument("--mixed-check-steps", type=int, default=100,
+                    help="jet workload: RK3 steps before the mixed-vs-FP64 error is taken")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus, sys.argv[1:])
     f3d = _package()
     if args.impl == "reference":
         return run_reference(args, f3d)
@@ -531,6 +706,8 @@ def main() -> int:
     ms = max_over_ranks(e0.elapsed_time(e1), dev)
     stages = 3 * args.steps
     cells = case.cells
+    launches_per_stage = dc.launches_per_stage()
+    stage_path, stage_config = dc.stage_kernels(), dc.launched_config
     value = replica_rate(cells, stages, ms, world)
     stage_ms = ms / stages  # device time of one stage (all of its launches)
 
@@ -591,14 +768,28 @@ def main() -> int:
     achieved = balg * cells / (stage_ms / 1e3) / 1e9
     traffic = None
     if TRAFFIC.exists():
-        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}:{dc.launched_config}")
+        tr = json.loads(TRAFFIC.read_text()).get(f"{args.workload}:{args.precision}:{stage_config}")
         if tr:
             traffic = tr.get("bytes_per_stage")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "peak_source": "measured" if PEAKS.exists() else "fallback",
-            "kernel": dc.stage_kernels(), "b_alg_bytes_per_cell": balg,
+            "kernel": stage_path, "b_alg_bytes_per_cell": balg,
             "stage_ms": stage_ms}
+    # the compute roof of the plain FP64 stage: FP64 FLOPs per cell-stage (ncu instruction
+    # counts, committed under profiles/) at the measured rate, against the measured FP64 peak
+    counts = json.loads(FP64_COUNTS.read_text()) if FP64_COUNTS.exists() else {}
+    fc = counts.get(f"{args.workload}:{args.precision}")
+    if fc and prec == 0:
+        fpk = fp64_peak_tflops(f3d, dev)
+        fach = fc["flop_per_cell_stage"] * cells / (stage_ms / 1e3) / 1e12
+        roof["fp64"] = {"achieved": fach, "peak": fpk, "unit": "TFLOP/s",
+                        "frac": fach / fpk if fpk else None,
+                        "flop_per_cell_stage": fc["flop_per_cell_stage"],
+                        "peak_source": "measured (csrc/probe/fp64_peak.cu, this run)",
+                        "counts_source": counts.get("source")}
+        roof["limiter"] = ("neither roof: FP64 issue and latency at 16 of 64 warps per SM "
+                           "(profiles/fp64_counts_jet128x64x64.md)")
 
     cpu = None
     if not args.no_cpu:
@@ -607,13 +798,26 @@ def main() -> int:
                "sample": f"{args.cpu_stages} RK3 stages of the oracle on a "
                          f"{cc.nx}x{cc.ny}x{cc.nz} slab of the workload ({secs:.1f} s)"}
 
+    extras = {}
+    if world == 1 and args.workload == "jet256x128x128" and not args.no_extras:
+        del dc
+        torch.cuda.empty_cache()
+        extras["launch_sequence"] = launch_sequence_record(f3d, case, dev)
+        if prec == 0:
+            extras["mixed"] = mixed_record(f3d, case, dev, args.mixed_check_steps)
+        extras["ensemble64"] = ensemble_record(f3d, dev, 10)
+        extras["extras_note"] = (
+            "launch_sequence: the reference's ~30 launches per stage of 1:1 kernels on this jet; "
+            "mixed: the same jet in mixed precision; ensemble64: BASELINE config 4, batched "
+            "mixed precision vs the plain FP64 paths one case at a time")
+
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if prec == 0 else "f32/f64",
            "data": "synthetic (seeded jet on the wavy periodic mapping)",
            "config": {"workload": args.workload, "cells": cells, "species": ns,
-                      "precision": args.precision, "path": dc.stage_kernels(), "stage_config": dc.launched_config,
+                      "precision": args.precision, "path": stage_path, "stage_config": stage_config,
                       "l2": "inputs larger than L2 (state ~%.1f GB per replica)" % (
                           (35 + 3 * ns) * case.Q[0].size * 8 / 1e9),
                       "parallelism": f"replicas x{world}"},
@@ -623,7 +827,7 @@ def main() -> int:
                    "calls": "DeviceCase.advance_from_host, one RK3 step per call, independent "
                             f"calls rotating over {E2E_LANES} cases on {E2E_LANES} streams",
                    "serial_one_stream": e2e_serial},
-           "gpu_launches": stages * dc.launches_per_stage()}
+           "gpu_launches": stages * launches_per_stage, **extras}
     print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()

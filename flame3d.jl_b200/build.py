@@ -75,7 +75,25 @@ def compile_one(src: Path, verbose_ptxas: bool) -> Path:
     return obj
 
 
+PROBE_SRC = CSRC / "probe" / "fp64_peak.cu"
+PROBE_LIB = HERE / "libflame3d_probe.so"
+
+
+def build_probe(force: bool = False) -> Path:
+    """libflame3d_probe.so: the FP64 FMA throughput probe bench.py measures the compute roof
+    with (kept out of the reference-facing library)."""
+    if not force and PROBE_LIB.exists() and PROBE_LIB.stat().st_mtime > PROBE_SRC.stat().st_mtime:
+        return PROBE_LIB
+    cmd = [nvcc(), *host_compiler(), *ARCH, *COMMON, "-shared", str(PROBE_SRC), "-o",
+           str(PROBE_LIB)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {PROBE_SRC.name}:\n{r.stdout}\n{r.stderr}")
+    return PROBE_LIB
+
+
 def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
+    build_probe(force)
     if not force and not needs_build():
         return LIB
     BUILD.mkdir(exist_ok=True)

@@ -626,8 +626,11 @@ def route(requests: list[SolveRequest], n_replicas: int, cost=None) -> list[list
 
 
 class MultiServer:
-    """One Server per GPU, requests routed up front by `route`; replicas share nothing (no
-    data-path collective), each runs its own stream of arrivals in its own host thread."""
+    """One Server per GPU; replicas share nothing (no data-path collective), each runs its own
+    stream of arrivals in its own host thread.  Requests are assigned by `route` before the
+    replicas start: an online rule (a request's replica depends only on the requests that
+    arrived before it, never on later ones), so it is the assignment a router that sees each
+    request at its arrival would make, but it does not look at how far each replica has got."""
 
     def __init__(self, devices, **server_kwargs):
         self.servers = [Server(d, **server_kwargs) for d in devices]

@@ -59,3 +59,32 @@ def test_single_process_is_its_own_max():
     b = _bench()
     assert b.max_over_ranks(7.5) == 7.5
     assert b.replica_rate(100, 3, 1.0, 1) == 100 * 3 / 1e-3 / 1e6
+
+
+def test_gpus_flag_self_launches_gloo_ranks():
+    """`bench.py --gpus 2` without torchrun starts two ranks itself (torch.distributed.run on
+    127.0.0.1).  The reference arm needs no GPU: its ranks meet in a gloo group, rank 0 alone
+    runs the oracle and prints one line with the N it ran under."""
+    import json
+    import subprocess
+    import sys
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    env["OMP_NUM_THREADS"] = "2"
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus",
+                        "2", "--workload", "tgv64", "--steps", "1", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["value"] > 0 and line["config"]["step"].startswith("one RK3 step")
+
+
+def test_relaunch_command_is_torchrun_on_localhost():
+    b = _bench()
+    cmd = b.relaunch_cmd(4, ["--steps", "2"], port=29555)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr=127.0.0.1" in cmd
+    assert "--master-port=29555" in cmd and cmd[-2:] == ["--steps", "2"]
