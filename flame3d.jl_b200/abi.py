@@ -138,6 +138,8 @@ SIGNATURES = {
     "flame_batch_create": [C.POINTER(C.c_void_p), C.POINTER(FlameCaseDesc), I, I, P, C.c_size_t,
                            S],
     "flame_batch_stage": [P, S, I, I],
+    "flame_batch_status": [P, S],
+    "flame_batch_test_stall": [P, I],
     "flame_batch_destroy": [P],
     "flame_last_error": [C.c_char_p, C.c_size_t],
     "flame_version": [],

@@ -3,8 +3,9 @@
 A `Batch` groups `DeviceCase`s that use the pencil configuration (each owns its state, metrics
 and scratch).  Two modes:
 
-* "persistent": flame_batch_* in the C ABI; one stage is four persistent launches per
-  species-count group over a (case, block) work list, whatever the number of cases;
+* "persistent": flame_batch_* in the C ABI; one stage is two persistent launches per chunk
+  of up to 20 cases of one species count, over a (case, block) work list of every phase of
+  every case (device counters order a case's phases; `status()` reports a wait that ran out);
 * "graph": every case's own launch chain (prep, z, y, x sweeps per stage) on one of several
   streams, forked and joined inside one CUDA graph, so the chains of small cases run side by
   side on the GPU and every kernel keeps its parameters in the constant bank.
@@ -159,6 +160,12 @@ class Batch:
                     p ^= 1
             self.graphs[par] = g
         torch.cuda.synchronize(self.device)
+
+    def status(self) -> None:
+        """Raises FlameError(FLAME_ETIMEOUT) if a persistent stage's bounded wait ran out since
+        the last call (synchronizes the stream); nothing to check in graph mode."""
+        if self.handle:
+            abi.check(self.lib, self.lib.flame_batch_status(self.handle, C.c_void_p(self.stream)))
 
     def close(self) -> None:
         self.graphs.clear()

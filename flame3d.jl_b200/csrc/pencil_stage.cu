@@ -134,9 +134,9 @@ __device__ __forceinline__ CT ldg(const T *p, int i) {
 }
 
 // ----------------------------------------------------------------------------------- prep
-template <int NS, typename QT>
+template <int NS, typename QT, int PTS = 256>
 __device__ __forceinline__ void prep_block(const Args<QT> &A, int bid) {
-    const int c = bid * 256 + threadIdx.x;
+    const int c = bid * PTS + threadIdx.x;
     if (c >= A.np) return;
     const int gx = c % A.tx, gy = (c / A.tx) % A.ty, gz = c / A.sz;
     const QT *P = A.Qi + 4 * A.np;
@@ -558,9 +558,9 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
 // (configuration 4: the FP64 finish then runs at full occupancy, apart from the sweep's
 // registers and shared memory).  Both form (R + R2) + rhs the same way, so they agree bit for
 // bit.
-template <int NS, typename QT, typename CT, bool FIN = true, bool MIXD = false>
+template <int NS, typename QT, typename CT, bool FIN = true, bool MIXD = false,
+          int WPB = Wpb<0>::value>
 __device__ __forceinline__ void x_block(const Args<QT> &A, int bid, unsigned char *smem_raw) {
-    constexpr int WPB = Wpb<0>::value;
     using SL = Slots<NS>;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     CT *S = reinterpret_cast<CT *>(smem_raw) + warp * SL::N * 32;
@@ -777,49 +777,138 @@ __global__ void __launch_bounds__(Staged<NS, CT, PART, MIXD>::COLS * 32)
 }
 
 // ---------------------------------------------------------------------- batched, persistent
-// The same sweeps over many independent cases: a persistent grid walks a work list of
-// (case, block) items; off[c] is the first item of case c (off[n] = total).  Per-case
-// descriptors live in device memory.  Cases never read each other's data, so a case's result
-// does not depend on which other cases share the batch.
-__device__ __forceinline__ int case_of(const int *off, int n, int item) {
-    int lo = 0, hi = n - 1;  // largest c with off[c] <= item
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= item) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
+// Two persistent launches per chunk of cases (one species count, configuration 3) and stage.
+// A work list holds, in this order, the prep blocks, z-sweep blocks and y-sweep blocks of all
+// the chunk's cases, then their x-sweep blocks (which finish the stage); item -> (case, block)
+// comes from a precomputed table.  k_batch_sweeps takes the first three phases' items in list
+// order from an atomic counter, so an item only ever waits for items taken before it: a case's
+// sweep item waits until the case's prep items are done (a counter in device memory; every wait
+// bounded: on timeout the batch's error word is set, the item is skipped and every later wait
+// gives up at once; flame_batch_status reports FLAME_ETIMEOUT).  k_batch_x follows on the
+// stream, so the stream orders the x items after every sweep item, and each kernel keeps the
+// registers of its own phases.  Cases never read each other's data, so a case's result does
+// not depend on which other cases share the batch.
+struct BatchItem {
+    int c, b;  // case (index within the chunk), block within the case's phase
+};
 
-template <int NS, typename QT>
-__global__ void __launch_bounds__(256) k_prep_batch(const Args<QT> *cases, const int *off, int n) {
-    const int total = off[n];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
-        const int c = case_of(off, n, item);
-        prep_block<NS, QT>(cases[c], item - off[c]);
-    }
-}
+struct BatchLaunch {
+    const BatchItem *items;  // work list
+    const int4 *need;        // per case: prep, z, y, x items
+    int *next;               // item counters of the two kernels (zeroed before the launches)
+    int *done;               // per case: completed prep items (zeroed before the launch)
+    int *err;                // the batch's error word (FLAME_ETIMEOUT)
+    int p1, p2, p3, total;   // first z item, first y item, first x item, item count
+    int stall;               // test hook: case 0 waits for one prep item more than exists
+};
 
-template <int DIR, int PASS, int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Staged<NS, CT>::COLS * 32)
-    k_staged_batch(const Args<QT> *cases, const int *off, int n) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int total = off[n];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
-        const int c = case_of(off, n, item);
-        staged_block<DIR, PASS, NS, QT, CT>(cases[c], item - off[c], smem_raw);
-        __syncthreads();  // the next item overwrites the staged columns
+constexpr int kWaitSpins = 1 << 22;  // x 128 ns: about half a second per wait
+
+// Spins (thread 0) until *count >= target; false if the batch already failed or the bound ran
+// out (then the error word is set).
+__device__ __forceinline__ bool wait_count(const int *count, int target, int *err) {
+    for (int i = 0; i < kWaitSpins; ++i) {
+        if (*(volatile const int *)err) return false;
+        if (*(volatile const int *)count >= target) {
+            __threadfence();  // acquire: the counted items' writes are visible from here on
+            return true;
+        }
+        __nanosleep(128);
     }
+    atomicExch(err, FLAME_ETIMEOUT);
+    return false;
 }
 
 template <int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(Wpb<0>::value * 32)
-    k_x_batch(const Args<QT> *cases, const int *off, int n) {
+struct BatchShape {
+    using ST = Staged<NS, CT>;
+    static constexpr int COLS = ST::COLS;
+    static constexpr int NT = ST::COLS * 32;  // threads of a sweep block (prep, z, y items)
+    static constexpr int XW = Wpb<0>::value;  // pencils of an x item (its warps)
+    static constexpr size_t SMEM = sizeof(CT) * ST::STRIDE * ST::COLS;
+    static constexpr size_t SMEM_X = smem_bytes<NS, CT, XW>();
+};
+
+constexpr int kPrepPerThread = 4;  // points each thread of a prep item handles
+
+// The descriptors of the cases a launch advances, in constant memory: copied (device to device)
+// before each launch, so the kernels read them through the constant cache as the stand-alone
+// kernels read their parameters (a descriptor read from shared or global memory costs a load
+// for every field, and from global memory the compiler must also assume that stores alias it).
+// One table per device context: persistent batches on one device run one after the other.
+constexpr int kConstCases = 20;
+__constant__ __align__(16) unsigned char c_batch_args[kConstCases * sizeof(Args<double>)];
+static_assert(sizeof(Args<double>) == sizeof(Args<float>), "one table for both precisions");
+
+template <typename QT>
+__device__ __forceinline__ const Args<QT> &batch_args(int c) {
+    return reinterpret_cast<const Args<QT> *>(c_batch_args)[c];
+}
+
+// Prep, z-sweep and y-sweep items (list positions [0, L.p3)): a sweep item first waits until
+// its case's prep items are done.  Thread 0 takes the next item from the counter while the
+// block works on the current one.
+template <int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(BatchShape<NS, QT, CT>::NT)
+    k_batch_sweeps(const __grid_constant__ BatchLaunch L) {
+    using BS = BatchShape<NS, QT, CT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int total = off[n];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
-        const int c = case_of(off, n, item);
-        x_block<NS, QT, CT>(cases[c], item - off[c], smem_raw);
-        __syncwarp();  // each warp reuses only its own slots
+    __shared__ int s_item, s_next, s_ok;
+    if (threadIdx.x == 0) s_next = atomicAdd(L.next, 1);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = s_next;
+        __syncthreads();
+        const int item = s_item;
+        if (item >= L.p3) return;
+        const BatchItem it = L.items[item];
+        const int ph = item < L.p1 ? 0 : item < L.p2 ? 1 : 2;
+        if (threadIdx.x == 0) {
+            s_next = atomicAdd(L.next, 1);  // in flight while the item runs
+            s_ok = ph == 0 || wait_count(L.done + 4 * it.c,
+                                         L.need[it.c].x + (L.stall && it.c == 0), L.err);
+        }
+        __syncthreads();
+        const Args<QT> &A = batch_args<QT>(it.c);
+        if (s_ok) {
+            if (ph == 0) {
+#pragma unroll
+                for (int k = 0; k < kPrepPerThread; ++k)
+                    prep_block<NS, QT, BS::NT>(A, it.b * kPrepPerThread + k);
+            } else if (ph == 1) {
+                staged_block<2, 0, NS, QT, CT>(A, it.b, smem_raw);
+            } else {
+                staged_block<1, 1, NS, QT, CT>(A, it.b, smem_raw);
+            }
+        }
+        __syncthreads();  // the item's writes are done and its shared memory is free
+        if (threadIdx.x == 0 && ph == 0) {
+            __threadfence();  // release: publish the prep block's writes before counting it
+            atomicAdd(L.done + 4 * it.c, 1);
+        }
+    }
+}
+
+// x-sweep items (list positions [L.p3, L.total)), launched after k_batch_sweeps on the same
+// stream, so all of every case's z and y items are done: they finish the stage.  They take
+// items from a second counter (L.next[1]), in the same way.
+template <int NS, typename QT, typename CT>
+__global__ void __launch_bounds__(BatchShape<NS, QT, CT>::XW * 32)
+    k_batch_x(const __grid_constant__ BatchLaunch L) {
+    using BS = BatchShape<NS, QT, CT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item, s_next;
+    if (threadIdx.x == 0) s_next = L.p3 + atomicAdd(L.next + 1, 1);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = s_next;
+        __syncthreads();
+        const int item = s_item;
+        if (item >= L.total) return;
+        const BatchItem it = L.items[item];
+        if (threadIdx.x == 0) s_next = L.p3 + atomicAdd(L.next + 1, 1);
+        if (!*(volatile const int *)L.err)
+            x_block<NS, QT, CT, true, false, BS::XW>(batch_args<QT>(it.c), it.b, smem_raw);
     }
 }
 
@@ -974,19 +1063,26 @@ extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
 }
 
 // ============================================================================= batches
-// A batch advances many independent periodic cases per stage with the persistent kernels above:
-// per species count one group, per group and stage four launches (prep, z, y, x).  Descriptors
-// and work lists for the three stages and both in/out parities are uploaded once, into device
-// workspace the caller owns, so flame_batch_stage issues kernel launches only.
+// A batch advances many independent cases per stage: the cases are grouped by species count and
+// the groups cut into chunks of at most kConstCases cases; per chunk and stage a copy of the
+// chunk's descriptors into the constant table, a memset of its counters and two persistent
+// launches, k_batch_sweeps (prep, z, y items) and k_batch_x (the finishing x items).
+// Descriptors for the three stages and both in/out parities, the work lists and the per-case
+// item counts are uploaded once, into device workspace the caller owns, so flame_batch_stage
+// issues copies, memsets and launches only (capturable as a CUDA graph).
+#include <algorithm>
+
 namespace flame {
 namespace pencil {
 
-struct BatchGroup {
+struct BatchChunk {
     int ns = 0, n = 0;
-    const void *args[6] = {};  // device Args arrays, index (stage - 1) * 2 + parity
-    const int *off[4] = {};    // device work-list offsets: prep, z, y, x
-    int total[4] = {};
-    int grid[4] = {};          // persistent grid sizes
+    const void *args[6] = {};    // device Args arrays of the chunk, index (stage - 1) * 2 + parity
+    const BatchItem *items = nullptr;
+    const int4 *need = nullptr;  // per case: prep, z, y, x items
+    int *counters = nullptr;     // item counters (ints 0, 1) and per case done[4], from int 4 on
+    int p1 = 0, p2 = 0, p3 = 0, total = 0;
+    int grid = 1, grid_x = 1;    // persistent blocks of the two kernels
 };
 
 }  // namespace pencil
@@ -994,8 +1090,9 @@ struct BatchGroup {
 
 struct FlameBatch {
     int precision = 0;
-    int ngroups = 0;
-    flame::pencil::BatchGroup g[FLAME_MAX_NS];
+    int *err = nullptr;  // device error word (FLAME_ETIMEOUT)
+    int stall = 0;       // test hook (flame_batch_test_stall)
+    std::vector<flame::pencil::BatchChunk> chunks;
 };
 
 namespace flame {
@@ -1006,71 +1103,92 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 template <typename QT>
 size_t args_size() { return sizeof(Args<QT>); }
 
-inline void case_items(const FlameGrid &g, int ns, int precision, int items[4]) {
-    const int tx = g.nx + 2 * g.ng, ty = g.ny + 2 * g.ng, tz = g.nz + 2 * g.ng;
-    const int np = tx * ty * tz;
-    const int cols = staged_cols(ns, precision == 0 ? 8 : 4);  // Staged<NS, CT>::COLS
+// Items of one case in each phase (prep, z, y, x), for a chunk whose sweep blocks have `nt`
+// threads and `cols` staged columns, and whose x items hold `xw` pencils.
+inline void case_items(const FlameGrid &g, int cols, int nt, int xw, int items[4]) {
+    const long long tx = g.nx + 2LL * g.ng, ty = g.ny + 2LL * g.ng, tz = g.nz + 2LL * g.ng;
+    const long long np = tx * ty * tz;
     const int nxb = (g.nx + cols - 1) / cols;
-    items[0] = (np + 255) / 256;
+    items[0] = (int)((np + (long long)nt * kPrepPerThread - 1) / ((long long)nt * kPrepPerThread));
     items[1] = nxb * ((g.nz + OWN - 1) / OWN) * g.ny;  // z sweep
     items[2] = nxb * ((g.ny + OWN - 1) / OWN) * g.nz;  // y sweep
     const long long warps = (long long)g.ny * g.nz * ((g.nx + OWN - 1) / OWN);
-    items[3] = (int)((warps + Wpb<0>::value - 1) / Wpb<0>::value);
+    items[3] = (int)((warps + xw - 1) / xw);
 }
 
 template <int NS, typename QT, typename CT>
-int batch_grids(BatchGroup &bg) {
-    int dev = 0, sms = 0;
+void batch_shape(int &cols, int &nt) {
+    cols = BatchShape<NS, QT, CT>::COLS;
+    nt = BatchShape<NS, QT, CT>::NT;
+}
+
+template <int NS, typename QT, typename CT>
+int batch_grid(BatchChunk &bc) {
+    using BS = BatchShape<NS, QT, CT>;
+    int dev = 0, sms = 0, occ = 0, occx = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    using ST = Staged<NS, CT>;
-    const size_t sm_st = sizeof(CT) * ST::STRIDE * ST::COLS;
-    const size_t sm_x = smem_bytes<NS, CT, Wpb<0>::value>();
-    static bool d0[64] = {}, d1[64] = {}, d2[64] = {};
-    if (int e = set_smem(k_staged_batch<2, 0, NS, QT, CT>, sm_st, d0)) return e;
-    if (int e = set_smem(k_staged_batch<1, 1, NS, QT, CT>, sm_st, d1)) return e;
-    if (int e = set_smem(k_x_batch<NS, QT, CT>, sm_x, d2)) return e;
-    int occ[4] = {0, 0, 0, 0};
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_prep_batch<NS, QT>, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_staged_batch<2, 0, NS, QT, CT>,
-                                                  ST::COLS * 32, sm_st);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_staged_batch<1, 1, NS, QT, CT>,
-                                                  ST::COLS * 32, sm_st);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_x_batch<NS, QT, CT>,
-                                                  Wpb<0>::value * 32, sm_x);
-    for (int k = 0; k < 4; ++k) {
-        const int cap = sms * (occ[k] > 0 ? occ[k] : 1);
-        bg.grid[k] = bg.total[k] < cap ? bg.total[k] : cap;
-        if (bg.grid[k] < 1) bg.grid[k] = 1;
-    }
+    static bool d0[64] = {}, d1[64] = {};
+    if (int e = set_smem(k_batch_sweeps<NS, QT, CT>, BS::SMEM, d0)) return e;
+    if (int e = set_smem(k_batch_x<NS, QT, CT>, BS::SMEM_X, d1)) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_sweeps<NS, QT, CT>, BS::NT,
+                                                  BS::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occx, k_batch_x<NS, QT, CT>, BS::XW * 32,
+                                                  BS::SMEM_X);
+    const int cap = sms * (occ > 0 ? occ : 1), capx = sms * (occx > 0 ? occx : 1);
+    bc.grid = std::max(1, std::min(bc.p3, cap));
+    bc.grid_x = std::max(1, std::min(bc.total - bc.p3, capx));
     return flame_check_launch("flame_batch_create");
 }
 
 template <int NS, typename QT, typename CT>
-int batch_launch(const BatchGroup &bg, cudaStream_t s, int stage, int parity) {
-    const Args<QT> *a = static_cast<const Args<QT> *>(bg.args[(stage - 1) * 2 + parity]);
-    using ST = Staged<NS, CT>;
-    const size_t sm_st = sizeof(CT) * ST::STRIDE * ST::COLS;
-    const size_t sm_x = smem_bytes<NS, CT, Wpb<0>::value>();
-    k_prep_batch<NS, QT><<<bg.grid[0], 256, 0, s>>>(a, bg.off[0], bg.n);
-    k_staged_batch<2, 0, NS, QT, CT><<<bg.grid[1], ST::COLS * 32, sm_st, s>>>(a, bg.off[1], bg.n);
-    k_staged_batch<1, 1, NS, QT, CT><<<bg.grid[2], ST::COLS * 32, sm_st, s>>>(a, bg.off[2], bg.n);
-    k_x_batch<NS, QT, CT><<<bg.grid[3], Wpb<0>::value * 32, sm_x, s>>>(a, bg.off[3], bg.n);
+int batch_launch(const BatchChunk &bc, cudaStream_t s, int stage, int parity, int *err,
+                 int stall) {
+    using BS = BatchShape<NS, QT, CT>;
+    cudaError_t ce = cudaMemcpyToSymbolAsync(c_batch_args, bc.args[(stage - 1) * 2 + parity],
+                                             sizeof(Args<QT>) * (size_t)bc.n, 0,
+                                             cudaMemcpyDeviceToDevice, s);
+    if (ce == cudaSuccess)
+        ce = cudaMemsetAsync(bc.counters, 0, sizeof(int) * (4 + 4 * (size_t)bc.n), s);
+    if (ce != cudaSuccess)
+        return flame_fail(FLAME_ELAUNCH, "flame_batch_stage: %s", cudaGetErrorString(ce));
+    BatchLaunch L;
+    L.items = bc.items;
+    L.need = bc.need;
+    L.next = bc.counters;
+    L.done = bc.counters + 4;
+    L.err = err;
+    L.p1 = bc.p1, L.p2 = bc.p2, L.p3 = bc.p3, L.total = bc.total;
+    L.stall = stall;
+    k_batch_sweeps<NS, QT, CT><<<bc.grid, BS::NT, BS::SMEM, s>>>(L);
+    if (int e = flame_check_launch("flame_batch_stage")) return e;
+    k_batch_x<NS, QT, CT><<<bc.grid_x, BS::XW * 32, BS::SMEM_X, s>>>(L);
     return flame_check_launch("flame_batch_stage");
 }
 
+// what: 0 the chunk's block shape (cols, nt), 1 its persistent grids, 2 a stage launch
 template <typename QT, typename CT>
-int batch_dispatch(int what, BatchGroup &bg, cudaStream_t s, int stage, int parity) {
-    switch (bg.ns) {
-#define CASE(N)                                                             \
-    case N:                                                                 \
-        return what == 0 ? batch_grids<N, QT, CT>(bg)                       \
-                         : batch_launch<N, QT, CT>(bg, s, stage, parity);
+int batch_dispatch(int what, BatchChunk &bc, cudaStream_t s, int stage, int parity, int *err,
+                   int stall, int *cols, int *nt) {
+    switch (bc.ns) {
+#define CASE(N)                                                                   \
+    case N:                                                                       \
+        if (what == 0) return batch_shape<N, QT, CT>(*cols, *nt), FLAME_OK;       \
+        if (what == 1) return batch_grid<N, QT, CT>(bc);                          \
+        return batch_launch<N, QT, CT>(bc, s, stage, parity, err, stall);
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
 #undef CASE
         default:
-            return flame_fail(FLAME_EUNSUPPORTED, "flame_batch: ns=%d (1..9)", bg.ns);
+            return flame_fail(FLAME_EUNSUPPORTED, "flame_batch: ns=%d (1..9)", bc.ns);
     }
+}
+
+inline int batch_dispatch_p(int precision, int what, BatchChunk &bc, cudaStream_t s, int stage,
+                            int parity, int *err, int stall, int *cols = nullptr,
+                            int *nt = nullptr) {
+    return precision == 0
+               ? batch_dispatch<double, double>(what, bc, s, stage, parity, err, stall, cols, nt)
+               : batch_dispatch<float, float>(what, bc, s, stage, parity, err, stall, cols, nt);
 }
 
 template <typename QT>
@@ -1094,33 +1212,59 @@ void fill_args(std::vector<unsigned char> &host, size_t at, const FlameCaseDesc 
 
 namespace {
 
-// Group sizes and the byte layout of the workspace: per group, six descriptor arrays then four
-// work-list offset arrays, each aligned to 256 bytes.
+// Chunks (cases of one species count, at most kConstCases each) and the byte layout of the
+// workspace: the batch's error word, then per chunk six descriptor arrays, the work list, the
+// per-case counts and the counters, each aligned to 256 bytes.
+struct ChunkPlan {
+    int ns = 0, cols = 0, nt = 0;
+    std::vector<int> members;  // case indices
+    long long total = 0;
+    size_t args_at[6] = {}, items_at = 0, need_at = 0, counters_at = 0;
+};
+
 struct Layout {
-    int ngroups = 0;
-    int ns[FLAME_MAX_NS] = {}, count[FLAME_MAX_NS] = {};
-    size_t args_at[FLAME_MAX_NS][6] = {}, off_at[FLAME_MAX_NS][4] = {};
+    std::vector<ChunkPlan> chunks;
     size_t bytes = 0;
 };
 
 int plan_layout(const FlameCaseDesc *cases, int n, int precision, Layout &L) {
-    for (int i = 0; i < n; ++i) {
-        const int ns = cases[i].grid.ns;
-        int k = 0;
-        while (k < L.ngroups && L.ns[k] != ns) ++k;
-        if (k == L.ngroups) {
-            if (L.ngroups == FLAME_MAX_NS) return flame_fail(FLAME_EINVAL, "flame_batch: groups");
-            L.ns[L.ngroups++] = ns;
+    std::vector<int> nss;
+    for (int i = 0; i < n; ++i)
+        if (std::find(nss.begin(), nss.end(), cases[i].grid.ns) == nss.end())
+            nss.push_back(cases[i].grid.ns);
+    for (int ns : nss) {
+        flame::pencil::BatchChunk probe;
+        probe.ns = ns;
+        int cols = 0, nt = 0;
+        if (int e = flame::pencil::batch_dispatch_p(precision, 0, probe, nullptr, 1, 0, nullptr,
+                                                    0, &cols, &nt))
+            return e;
+        for (int i = 0; i < n; ++i) {
+            if (cases[i].grid.ns != ns) continue;
+            if (L.chunks.empty() || L.chunks.back().ns != ns ||
+                (int)L.chunks.back().members.size() == flame::pencil::kConstCases) {
+                L.chunks.emplace_back();
+                L.chunks.back().ns = ns, L.chunks.back().cols = cols, L.chunks.back().nt = nt;
+            }
+            ChunkPlan &c = L.chunks.back();
+            c.members.push_back(i);
+            int it[4];
+            flame::pencil::case_items(cases[i].grid, cols, nt, flame::pencil::Wpb<0>::value, it);
+            c.total += (long long)it[0] + it[1] + it[2] + it[3];
         }
-        ++L.count[k];
     }
     const size_t asz = precision == 0 ? flame::pencil::args_size<double>()
                                       : flame::pencil::args_size<float>();
-    size_t at = 0;
-    for (int k = 0; k < L.ngroups; ++k) {
-        for (int v = 0; v < 6; ++v) L.args_at[k][v] = at, at = flame::pencil::align256(at + asz * L.count[k]);
-        for (int w = 0; w < 4; ++w)
-            L.off_at[k][w] = at, at = flame::pencil::align256(at + sizeof(int) * (L.count[k] + 1));
+    using flame::pencil::align256;
+    size_t at = 256;  // the error word
+    for (ChunkPlan &c : L.chunks) {
+        if (c.total >= (1LL << 31))
+            return flame_fail(FLAME_EINVAL, "flame_batch: %lld work items in one chunk", c.total);
+        const size_t m = c.members.size();
+        for (int v = 0; v < 6; ++v) c.args_at[v] = at, at = align256(at + asz * m);
+        c.items_at = at, at = align256(at + sizeof(flame::pencil::BatchItem) * c.total);
+        c.need_at = at, at = align256(at + sizeof(int4) * m);
+        c.counters_at = at, at = align256(at + sizeof(int) * (4 + 4 * m));
     }
     L.bytes = at;
     return FLAME_OK;
@@ -1134,8 +1278,10 @@ int check_case(const FlameCaseDesc &c, int i) {
     if (c.grid.nx < FLAME_NG || c.grid.ny < FLAME_NG || c.grid.nz < FLAME_NG)
         return flame_fail(FLAME_EINVAL, "flame_batch: case %d extents must be >= %d", i, FLAME_NG);
     const long long np =
-        (long long)(c.grid.nx + 8) * (c.grid.ny + 8) * (c.grid.nz + 8);
-    if (np * 10 >= (1LL << 31)) return flame_fail(FLAME_EINVAL, "flame_batch: case %d too large", i);
+        ((long long)c.grid.nx + 8) * ((long long)c.grid.ny + 8) * ((long long)c.grid.nz + 8);
+    if (c.grid.nx > (1 << 20) || c.grid.ny > (1 << 20) || c.grid.nz > (1 << 20) ||
+        np * 10 >= (1LL << 31))
+        return flame_fail(FLAME_EINVAL, "flame_batch: case %d too large", i);
     const FlameStageBuffers &b = c.buf;
     if (!b.U || !b.Un || !b.Q_in || !b.Q_out || !b.rhoi_in || !b.rhoi_out || !b.rhon ||
         !b.trans_in || !b.trans_out || !b.scratch || !c.metrics.J || !c.metrics.dxidx)
@@ -1151,7 +1297,9 @@ int check_case(const FlameCaseDesc &c, int i) {
 }  // namespace
 
 extern "C" size_t flame_batch_workspace_bytes(const FlameCaseDesc *cases, int n, int precision) {
-    if (!cases || n < 1) return 0;
+    if (!cases || n < 1 || (precision != 0 && precision != 1)) return 0;
+    for (int i = 0; i < n; ++i)
+        if (check_case(cases[i], i)) return 0;
     Layout L;
     if (plan_layout(cases, n, precision, L)) return 0;
     return L.bytes;
@@ -1173,42 +1321,50 @@ extern "C" int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, 
     std::vector<unsigned char> host(L.bytes, 0);
     FlameBatch *B = new FlameBatch();
     B->precision = precision;
-    B->ngroups = L.ngroups;
     unsigned char *dev = static_cast<unsigned char *>(workspace);
+    B->err = reinterpret_cast<int *>(dev);
     const size_t asz = precision == 0 ? flame::pencil::args_size<double>()
                                       : flame::pencil::args_size<float>();
-    for (int k = 0; k < L.ngroups; ++k) {
-        flame::pencil::BatchGroup &bg = B->g[k];
-        bg.ns = L.ns[k];
-        bg.n = L.count[k];
-        std::vector<int> off[4];
-        for (int w = 0; w < 4; ++w) off[w].push_back(0);
-        int j = 0;
-        for (int i = 0; i < n; ++i) {
-            if (cases[i].grid.ns != bg.ns) continue;
+    using flame::pencil::BatchItem;
+    for (const ChunkPlan &cp : L.chunks) {
+        flame::pencil::BatchChunk bc;
+        bc.ns = cp.ns;
+        bc.n = (int)cp.members.size();
+        std::vector<int4> need(bc.n);
+        for (int j = 0; j < bc.n; ++j) {
+            const FlameCaseDesc &c = cases[cp.members[j]];
+            int it[4];
+            flame::pencil::case_items(c.grid, cp.cols, cp.nt, flame::pencil::Wpb<0>::value, it);
+            need[j] = make_int4(it[0], it[1], it[2], it[3]);
             for (int st = 1; st <= 3; ++st)
                 for (int par = 0; par < 2; ++par) {
-                    const size_t at = L.args_at[k][(st - 1) * 2 + par] + asz * j;
-                    if (precision == 0) flame::pencil::fill_args<double>(host, at, cases[i], st, par);
-                    else flame::pencil::fill_args<float>(host, at, cases[i], st, par);
+                    const size_t at = cp.args_at[(st - 1) * 2 + par] + asz * j;
+                    if (precision == 0) flame::pencil::fill_args<double>(host, at, c, st, par);
+                    else flame::pencil::fill_args<float>(host, at, c, st, par);
                 }
-            int items[4];
-            flame::pencil::case_items(cases[i].grid, bg.ns, precision, items);
-            for (int w = 0; w < 4; ++w) off[w].push_back(off[w].back() + items[w]);
-            ++j;
         }
-        for (int w = 0; w < 4; ++w) {
-            memcpy(host.data() + L.off_at[k][w], off[w].data(), sizeof(int) * off[w].size());
-            bg.off[w] = reinterpret_cast<const int *>(dev + L.off_at[k][w]);
-            bg.total[w] = off[w].back();
+        // work list: every case's prep items, then z, then y, then x items
+        BatchItem *items = reinterpret_cast<BatchItem *>(host.data() + cp.items_at);
+        long long w = 0;
+        int first[4] = {};
+        for (int ph = 0; ph < 4; ++ph) {
+            first[ph] = (int)w;
+            for (int j = 0; j < bc.n; ++j) {
+                const int cnt = ph == 0 ? need[j].x : ph == 1 ? need[j].y : ph == 2 ? need[j].z : need[j].w;
+                for (int b = 0; b < cnt; ++b) items[w++] = BatchItem{j, b};
+            }
         }
-        for (int v = 0; v < 6; ++v) bg.args[v] = dev + L.args_at[k][v];
-        const int e = precision == 0 ? flame::pencil::batch_dispatch<double, double>(0, bg, s, 1, 0)
-                                     : flame::pencil::batch_dispatch<float, float>(0, bg, s, 1, 0);
-        if (e) {
+        memcpy(host.data() + cp.need_at, need.data(), sizeof(int4) * bc.n);
+        for (int v = 0; v < 6; ++v) bc.args[v] = dev + cp.args_at[v];
+        bc.items = reinterpret_cast<const BatchItem *>(dev + cp.items_at);
+        bc.need = reinterpret_cast<const int4 *>(dev + cp.need_at);
+        bc.counters = reinterpret_cast<int *>(dev + cp.counters_at);
+        bc.p1 = first[1], bc.p2 = first[2], bc.p3 = first[3], bc.total = (int)w;
+        if (int e = flame::pencil::batch_dispatch_p(precision, 1, bc, s, 1, 0, B->err, 0)) {
             delete B;
             return e;
         }
+        B->chunks.push_back(bc);
     }
     cudaError_t ce = cudaMemcpyAsync(workspace, host.data(), L.bytes, cudaMemcpyHostToDevice, s);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
@@ -1225,12 +1381,32 @@ extern "C" int flame_batch_stage(FlameBatch *B, flame_stream_t s, int stage, int
     if (!B) return flame_fail(FLAME_EINVAL, "flame_batch_stage: NULL batch");
     if (stage < 1 || stage > 3 || (parity != 0 && parity != 1))
         return flame_fail(FLAME_EINVAL, "flame_batch_stage: stage=%d parity=%d", stage, parity);
-    for (int k = 0; k < B->ngroups; ++k) {
-        const int e = B->precision == 0
-                          ? flame::pencil::batch_dispatch<double, double>(1, B->g[k], s, stage, parity)
-                          : flame::pencil::batch_dispatch<float, float>(1, B->g[k], s, stage, parity);
-        if (e) return e;
-    }
+    for (flame::pencil::BatchChunk &bc : B->chunks)
+        if (int e = flame::pencil::batch_dispatch_p(B->precision, 2, bc, s, stage, parity, B->err,
+                                                    B->stall))
+            return e;
+    return FLAME_OK;
+}
+
+extern "C" int flame_batch_status(FlameBatch *B, flame_stream_t s) {
+    if (!B) return flame_fail(FLAME_EINVAL, "flame_batch_status: NULL batch");
+    int h = 0;
+    cudaError_t ce = cudaMemcpyAsync(&h, B->err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce == cudaSuccess && h) ce = cudaMemsetAsync(B->err, 0, sizeof(int), s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess)
+        return flame_fail(FLAME_ELAUNCH, "flame_batch_status: %s", cudaGetErrorString(ce));
+    if (h)
+        return flame_fail(FLAME_ETIMEOUT,
+                          "flame_batch_stage: a wait for another work item's completion ran out; "
+                          "the items after it were skipped and the cases' states are invalid");
+    return FLAME_OK;
+}
+
+extern "C" int flame_batch_test_stall(FlameBatch *B, int on) {
+    if (!B) return flame_fail(FLAME_EINVAL, "flame_batch_test_stall: NULL batch");
+    B->stall = on != 0;
     return FLAME_OK;
 }
 

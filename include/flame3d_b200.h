@@ -15,9 +15,11 @@
  *   - Every call is asynchronous on `stream` (NULL = legacy default stream) and returns
  *     FLAME_OK or an error code; flame_last_error() gives the message of the calling thread.
  *   - Global state of the library: a per-thread error string; per device, flags recording that
- *     a kernel's dynamic shared-memory limit has been raised (set once, never cleared); and,
- *     used only by flame_rk_stage_noalloc, a library-held scratch array with its per-device
- *     address cache (described at that entry point).  No call allocates device memory.
+ *     a kernel's dynamic shared-memory limit has been raised (set once, never cleared); the
+ *     persistent batch's constant-memory descriptor table (one per device, see flame_batch_*);
+ *     and, used only by flame_rk_stage_noalloc, a library-held scratch array with its
+ *     per-device address cache (described at that entry point).  No call allocates device
+ *     memory.
  *
  * The argument order after (grid, stream) is the argument order of the reference kernel each
  * entry point replaces, so a Julia `ccall` is a mechanical rewrite of the `@cuda` launch.
@@ -418,13 +420,20 @@ int flame_transport_boundary(const FlameGrid *g, flame_stream_t stream, const vo
 
 /* ---------------------------------------------------------------------------------------
  * Batches (no reference counterpart): many independent periodic cases, each with its own
- * grid, species count, thermodynamics, transport, dt and buffers, advanced together by the
- * pencil-sweep kernels.  A persistent grid per species-count group walks a (case, block) work
- * list; one stage is four launches per group.  Descriptors and work lists for all stages and
- * both in/out parities go once into caller-owned device workspace, so a captured CUDA graph of
+ * grid, species count, thermodynamics, transport (laws 0 and 1), dt and buffers, advanced
+ * together by persistent kernels (configuration 3).  Cases are grouped by species count and cut
+ * into chunks of at most 20; per chunk and stage the chunk's descriptors go into a constant-
+ * memory table and two persistent kernels run: the first takes the prep, z-sweep and y-sweep
+ * blocks of every case of the chunk in list order, a case's sweep blocks waiting on a device
+ * counter for that case's prep blocks; the second, after it on the stream, runs the x-sweep
+ * blocks, which finish the stage.  Every wait is bounded: when one runs out (about half a
+ * second) the batch's error word is set and the remaining items are skipped;
+ * flame_batch_status reports it.  The constant table is one per device: persistent batches on
+ * one device must not run concurrently.  Descriptors and work lists for all stages and both
+ * in/out parities go once into caller-owned device workspace, so a captured CUDA graph of
  * flame_batch_stage calls replays without host work.  parity 0 advances buf.*_in -> buf.*_out,
- * parity 1 the other way.  Every case needs buf.scratch (flame_stage_scratch_bytes).  A case's
- * result is the same as when it runs alone: cases share no data and no reduction.
+ * parity 1 the other way.  Every case needs buf.scratch (flame_stage_scratch_bytes).  A
+ * case's result is the same as when it runs alone: cases share no data and no reduction.
  * ------------------------------------------------------------------------------------- */
 typedef struct FlameCaseDesc {
     FlameGrid grid;
@@ -441,6 +450,13 @@ size_t flame_batch_workspace_bytes(const FlameCaseDesc *cases, int n, int precis
 int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, int n, int precision,
                        void *workspace, size_t bytes, flame_stream_t stream);
 int flame_batch_stage(FlameBatch *batch, flame_stream_t stream, int stage, int parity);
+/* Synchronizes `stream` and returns FLAME_ETIMEOUT (and clears it) if a wait of an earlier
+ * flame_batch_stage ran out, else FLAME_OK. */
+int flame_batch_status(FlameBatch *batch, flame_stream_t stream);
+/* Test hook: with on != 0, the next stages make the first case of every chunk wait for one
+ * more prep block than exists, a completion that never comes, so its waits run out and
+ * flame_batch_status reports FLAME_ETIMEOUT (a host-side injection; nothing faults). */
+int flame_batch_test_stall(FlameBatch *batch, int on);
 int flame_batch_destroy(FlameBatch *batch);
 
 /* Message of the last error on the calling thread; returns its length. */

@@ -12,7 +12,8 @@ oracle_regression.json
     norms and sampled values.  They are not reference outputs (the reference cannot run here);
     they freeze the oracle so an accidental edit of the restatement is caught.
 
-    python tests/golden/make_golden.py [--reference /path/to/Flame3D.jl]
+    python tests/golden/make_golden.py --reference /path/to/Flame3D.jl
+    (or FLAME3D_REFERENCE=/path/to/Flame3D.jl python tests/golden/make_golden.py)
 """
 from __future__ import annotations
 
@@ -83,9 +84,13 @@ def regression_fixture() -> dict:
 
 
 if __name__ == "__main__":
+    import os
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FLAME3D_REFERENCE"),
+                    help="checkout of Flame3D.jl (default: $FLAME3D_REFERENCE)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give the reference checkout: --reference PATH or FLAME3D_REFERENCE=PATH")
     (HERE / "up7_fdmcoeffs.json").write_text(json.dumps(up7_fixture(Path(a.reference)), indent=1))
     (HERE / "oracle_regression.json").write_text(json.dumps(regression_fixture(), indent=1))
     print("wrote", HERE / "up7_fdmcoeffs.json", HERE / "oracle_regression.json")

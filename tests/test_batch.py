@@ -150,3 +150,82 @@ def test_graph_batch_with_law2_case(f3d, cuda_ok):
     with pytest.raises(f3d.abi.FlameError) as e:
         B.Batch([S.DeviceCase(law2, tile=3)], mode="persistent")
     assert e.value.code == 5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_batch_agrees_with_configuration_3(f3d, cuda_ok, precision):
+    """The persistent kernels run configuration 3's prep, z, y and finishing x blocks from one
+    work list; each case ends where the stand-alone configuration 3 puts it, up to the
+    compiler's multiply-add contraction in a different kernel (1e-12 FP64, 1e-6 FP32, relative
+    L2 per field; species counts 1-6)."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d) + [f3d.taylor_green(n=12, ns=5, perturb=0.02, seed=56),
+                         f3d.random_curvilinear(n=10, ns=6, seed=57)]
+    batched = [S.DeviceCase(c, precision=precision, tile=3) for c in cases]
+    alone = [S.DeviceCase(c, precision=precision, tile=3) for c in cases]
+    b = B.Batch(batched, mode="persistent")
+    b.capture()
+    for _ in range(2):
+        b.step()
+        for dc in alone:
+            dc.step()
+    b.status()
+    tol = 1e-12 if precision == 0 else 1e-6
+    for x, y in zip(batched, alone):
+        for a, c in zip(_state(x), _state(y)):
+            for k in range(a.shape[0]):
+                n = np.linalg.norm(c[k].ravel())
+                assert np.linalg.norm((a[k] - c[k]).ravel()) <= tol * n, (x.case.name, k)
+    b.close()
+
+
+def test_persistent_batch_more_cases_than_one_chunk(f3d, cuda_ok):
+    """More cases of one species count than the constant descriptor table holds (20): the
+    batch runs them in chunks, and every case agrees with its stand-alone run."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = [f3d.taylor_green(n=8 + (i % 5), perturb=0.02, seed=100 + i) for i in range(23)]
+    batched = [S.DeviceCase(c, tile=3) for c in cases]
+    alone = [S.DeviceCase(c, tile=3) for c in cases]
+    b = B.Batch(batched, mode="persistent")
+    b.step()
+    b.status()
+    for dc in alone:
+        dc.step()
+    for x, y in zip(batched, alone):
+        U, V = x.conserved(), y.conserved()
+        assert np.linalg.norm((U - V).ravel()) <= 1e-12 * np.linalg.norm(V.ravel())
+    b.close()
+
+
+def test_persistent_wait_runs_out_and_reports(f3d, cuda_ok):
+    """A completion that never comes (flame_batch_test_stall): the waits give up after their
+    bound, the stage returns, flame_batch_status reports FLAME_ETIMEOUT once, and the batch and
+    the GPU stay usable; nothing faults or hangs."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)[:3]
+    dcs = [S.DeviceCase(c, tile=3) for c in cases]
+    b = B.Batch(dcs, mode="persistent")
+    f3d.abi.check(b.lib, b.lib.flame_batch_test_stall(b.handle, 1))
+    b.step()
+    with pytest.raises(f3d.abi.FlameError) as e:
+        b.status()
+    assert e.value.code == 3
+    b.status()  # reported once
+    f3d.abi.check(b.lib, b.lib.flame_batch_test_stall(b.handle, 0))
+    fresh = [S.DeviceCase(c, tile=3) for c in cases]
+    alone = [S.DeviceCase(c, tile=3) for c in cases]
+    b2 = B.Batch(fresh, mode="persistent")
+    b2.step()
+    b2.status()
+    for dc in alone:
+        dc.step()
+    for x, y in zip(fresh, alone):
+        for a, c in zip(_state(x), _state(y)):
+            for k in range(a.shape[0]):
+                n = np.linalg.norm(c[k].ravel())
+                assert np.linalg.norm((a[k] - c[k]).ravel()) <= 1e-12 * n
+    b.close()
+    b2.close()
