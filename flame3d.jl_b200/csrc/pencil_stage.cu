@@ -827,6 +827,12 @@ struct BatchShape {
     static constexpr int XW = Wpb<0>::value;  // pencils of an x item (its warps)
     static constexpr size_t SMEM = sizeof(CT) * ST::STRIDE * ST::COLS;
     static constexpr size_t SMEM_X = smem_bytes<NS, CT, XW>();
+    // x blocks per SM that the shared memory allows (228 KB, 1 KB reserved per block), as the
+    // register bound that lets them all be resident; in FP32, whose blocks are small, at most
+    // six (80 registers) up to three species and four (128) above, where fewer would spill
+    static constexpr int FIT_X = int((228 * 1024) / (SMEM_X + 1024));
+    static constexpr int CAP_X = sizeof(CT) == 8 ? 8 : (NS <= 3 ? 6 : 4);
+    static constexpr int MINB_X = FIT_X < 1 ? 1 : (FIT_X > CAP_X ? CAP_X : FIT_X);
 };
 
 constexpr int kPrepPerThread = 4;  // points each thread of a prep item handles
@@ -893,7 +899,7 @@ __global__ void __launch_bounds__(BatchShape<NS, QT, CT>::NT)
 // stream, so all of every case's z and y items are done: they finish the stage.  They take
 // items from a second counter (L.next[1]), in the same way.
 template <int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(BatchShape<NS, QT, CT>::XW * 32)
+__global__ void __launch_bounds__(BatchShape<NS, QT, CT>::XW * 32, BatchShape<NS, QT, CT>::MINB_X)
     k_batch_x(const __grid_constant__ BatchLaunch L) {
     using BS = BatchShape<NS, QT, CT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
