@@ -68,14 +68,16 @@ struct Args {
     FlameTransport tr;
 };
 
-// Shared-memory slots of one lane's point (CT each).
-template <int NS>
+// Shared-memory slots of one lane's point (CT each).  REUSE (the FP64 y and z sweeps): the
+// metrics are staged after the reconstruction has read the split fluxes, into their slots, so a
+// point needs ten slots fewer and three 8-column blocks fit on an SM.
+template <int NS, bool REUSE = false>
 struct Slots {
     static constexpr int FP = 0;                // F+ flow (5), F- flow (5), F+ sp (NS), F- sp (NS)
     static constexpr int VF = 10 + 2 * NS;
     static constexpr int Q4 = VF;               // u v w T
-    static constexpr int MET = Q4 + 4;          // 9 metrics + J
-    static constexpr int TR = MET + 10;         // μ λ D
+    static constexpr int MET = REUSE ? FP : Q4 + 4;    // 9 metrics + J
+    static constexpr int TR = REUSE ? Q4 + 4 : MET + 10;  // μ λ D
     static constexpr int RHO = TR + 3;
     static constexpr int Y = RHO + 1;           // NS
     static constexpr int DQ1 = Y + NS;          // tangential derivatives of u v w T along d+1
@@ -111,8 +113,8 @@ struct SpSlots {
 
 // PART 0: the whole face flux; PART 2: the species fluxes and the enthalpy-diffusion term of the
 // energy flux only (the flow part then runs as the NS = 0 instance of the same sweep).
-template <int NS, int PART, bool MIXD = false>
-using SlotsOf = std::conditional_t<PART == 2, SpSlots<NS, MIXD>, Slots<NS>>;
+template <int NS, int PART, bool MIXD = false, bool REUSE = false>
+using SlotsOf = std::conditional_t<PART == 2, SpSlots<NS, MIXD>, Slots<NS, REUSE>>;
 
 template <int NS, typename CT, int WPB>
 constexpr size_t smem_bytes() {
@@ -194,9 +196,9 @@ __device__ __forceinline__ void transport_point(const FlameThermo &th, const Fla
 
 // ---- phase A: everything the faces of a pencil need from one point, into the point's
 // column of shared memory (slot stride 32).  l is the point's position along the pencil.
-template <int DIR, int NS, typename QT, typename CT>
+template <int DIR, int NS, typename QT, typename CT, bool REUSE = false>
 __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int g) {
-    using SL = Slots<NS>;
+    using SL = Slots<NS, REUSE>;
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
     const int np = A.np;
     const int s1 = D1 == 0 ? 1 : (D1 == 1 ? A.sy : A.sz);
@@ -258,8 +260,10 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
         }
     }
     SV(SL::Q4 + 0) = u, SV(SL::Q4 + 1) = v, SV(SL::Q4 + 2) = w, SV(SL::Q4 + 3) = T;
+    if constexpr (!REUSE) {  // REUSE: staged later, into the split slots (stage_metrics)
 #pragma unroll
-    for (int m = 0; m < 10; ++m) SV(SL::MET + m) = mv[m];
+        for (int m = 0; m < 10; ++m) SV(SL::MET + m) = mv[m];
+    }
 #pragma unroll
     for (int m = 0; m < 3; ++m) SV(SL::TR + m) = CT(A.Ti[g + m * np]);
     SV(SL::RHO) = rho;
@@ -291,10 +295,14 @@ __device__ __forceinline__ void point_phase(const Args<QT> &A, CT *S, int l, int
 // point l in the transport fields (field 2 + n holds D_n) and dstep is the pencil's stride, so
 // point l - 1 is Dk - dstep.  The other laws use the one D of the shared-memory slots and
 // compile without the per-species loads.
-template <int DIR, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
+// MODE 0: the whole face.  With the REUSE slots the face runs in two calls, between which the
+// metrics overwrite the split fluxes: MODE 1 reconstructs every flux into G, MODE 2 subtracts
+// the viscous and diffusion fluxes from it (the same operations in the same order as MODE 0).
+template <int DIR, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false,
+          int MODE = 0, bool REUSE = false>
 __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l, CT *G,
                                            const QT *Dk, int dstep) {
-    using SL = SlotsOf<NS, PART, MIXD>;
+    using SL = SlotsOf<NS, PART, MIXD, REUSE>;
     constexpr int GS = PART == 2 ? 0 : 5;  // G index of species 0
     constexpr int D1 = Dir<DIR>::D1, D2 = Dir<DIR>::D2;
     const CT h = CT(0.5), c23 = CT(2.0 / 3.0), c12 = CT(1.0 / 12.0);
@@ -308,9 +316,14 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
         pv[6] = mv[6] = CT(0);
         return hybrid_face_fast<CT>(pv, mv, phif);
     };
-    if constexpr (PART != 2) {
+    if constexpr (PART != 2 && MODE != 2) {
 #pragma unroll
         for (int n = 0; n < 5; ++n) G[n] = recon(n, 5 + n);
+    }
+    if constexpr (MODE == 1) {
+#pragma unroll
+        for (int n = 0; n < NS; ++n) G[GS + n] = recon(SL::SPP + n, SL::SPM + n);
+        return;
     }
     CT met[9];
 #pragma unroll
@@ -359,7 +372,8 @@ __device__ __forceinline__ void face_phase(const Args<QT> &A, const CT *S, int l
             const CT Yf = diffusion(n, Vx, Vy, Vz);
             const CT hn = CT(h_spec(A.th, n, Td, T2, T3, T4, T5));
             const CT V1 = Vx - sum1 * Yf, V2 = Vy - sum2 * Yf, V3 = Vz - sum3 * Yf;
-            G[GS + n] = recon(SL::SPP + n, SL::SPM + n) - (V1 * md[0] + V2 * md[1] + V3 * md[2]);
+            const CT gi = MODE == 2 ? G[GS + n] : recon(SL::SPP + n, SL::SPM + n);
+            G[GS + n] = gi - (V1 * md[0] + V2 * md[1] + V3 * md[2]);
             fh1 += V1 * hn, fh2 += V2 * hn, fh3 += V3 * hn;
         }
     }
@@ -672,13 +686,22 @@ constexpr int staged_cols(int ns, size_t csz) {
 template <int NS, typename CT, int PART = 0, bool MIXD = false>
 struct Staged {
     static_assert(Slots<NS>::N == slots_of(NS), "slots_of must follow Slots");
-    static constexpr int NSLOT = SlotsOf<NS, PART, MIXD>::N;
+    // FP64 sweeps with one or two species stage the metrics into the split slots once the
+    // reconstruction is done: ten slots fewer per point let three blocks share an SM (more
+    // species would not fit three blocks anyway)
+    static constexpr bool REUSE = sizeof(CT) == 8 && PART == 0 && NS >= 1 && NS <= 2;
+    static constexpr int NSLOT = SlotsOf<NS, PART, MIXD, REUSE>::N;
     static constexpr int STRIDE = NSLOT * 32 + 1;  // padded column region (bank spread)
     // (the species sweep in 8-column blocks capped at three per SM measured 7-12 % slower in
     // mixed precision: the register cap spills)
     static constexpr int COLS =
         PART == 2 ? (sizeof(CT) * NSLOT * 33 * 16 <= 200 * 1024 ? 16 : 8)
                   : staged_cols(NS, sizeof(CT));
+    static constexpr size_t SMEM = sizeof(CT) * STRIDE * COLS;
+    // three 8-column FP64 blocks per SM when their shared memory fits (228 KB per SM, 1 KB
+    // reserved per block): at most 80 registers; otherwise no bound
+    static constexpr int MINB =
+        (sizeof(CT) == 8 && COLS == 8 && 3 * (SMEM + 1024) <= 228 * 1024) ? 3 : 1;
 };
 
 // y or z sweep (DIR 1, 2).  The block stages the points of COLS neighbouring pencils with
@@ -689,7 +712,8 @@ template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, boo
 __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsigned char *smem_raw) {
     constexpr int COLS = Staged<NS, CT, PART, MIXD>::COLS;
     constexpr int STRIDE = Staged<NS, CT, PART, MIXD>::STRIDE;
-    using SL = SlotsOf<NS, PART, MIXD>;
+    constexpr bool REUSE = Staged<NS, CT, PART, MIXD>::REUSE;
+    using SL = SlotsOf<NS, PART, MIXD, REUSE>;
     constexpr int NG_OUT = PART == 2 ? NS + 1 : 5 + NS;  // face values a lane produces
     CT *base = reinterpret_cast<CT *>(smem_raw);
     const int n_along = DIR == 1 ? A.ny : A.nz;
@@ -712,6 +736,7 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
         }
     }
     // ---- phase A, x-fastest: thread -> (column cx, pencil position l)
+    int gA;  // the thread's phase-A point
     {
         const int cx = tid % COLS, l = tid / COLS;
         const int x = clampi(xb * COLS + cx, 0, A.nx - 1);
@@ -720,11 +745,11 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
         const int gx = x + A.ng;
         const int gy = DIR == 1 ? ga : c2 + A.ng;
         const int gz = DIR == 1 ? c2 + A.ng : ga;
+        gA = gx + A.sy * gy + A.sz * gz;
         if constexpr (PART == 2)
-            species_point_phase<DIR, NS, QT, CT, MIXD>(A, base + cx * STRIDE, l,
-                                                       gx + A.sy * gy + A.sz * gz);
+            species_point_phase<DIR, NS, QT, CT, MIXD>(A, base + cx * STRIDE, l, gA);
         else
-            point_phase<DIR, NS, QT, CT>(A, base + cx * STRIDE, l, gx + A.sy * gy + A.sz * gz);
+            point_phase<DIR, NS, QT, CT, REUSE>(A, base + cx * STRIDE, l, gA);
     }
     __syncthreads();
     // ---- phase B, one warp per pencil (column)
@@ -733,13 +758,33 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
     const int a = seg * OWN - 3 + lane;
     CT G[NG_OUT];
     const bool face = lane >= 3 && lane <= 3 + OWN && a <= n_along;
-    if (face) {
-        // the lane's point in the transport fields (per-species D_k of law 2)
-        const int gxw = clampi(xb * COLS + warp, 0, A.nx - 1) + A.ng, gaw = a + A.ng;
-        const int gl = gxw + (DIR == 1 ? A.sy * gaw + A.sz * (c2 + A.ng)
-                                       : A.sy * (c2 + A.ng) + A.sz * gaw);
+    // the lane's point in the transport fields (per-species D_k of law 2)
+    const int gxw = clampi(xb * COLS + warp, 0, A.nx - 1) + A.ng, gaw = a + A.ng;
+    const int gl = gxw + (DIR == 1 ? A.sy * gaw + A.sz * (c2 + A.ng)
+                                   : A.sy * (c2 + A.ng) + A.sz * gaw);
+    if constexpr (REUSE) {
+        // the reconstruction, then every warp is done with the split fluxes: the x-fastest
+        // threads stage their point's metrics into those slots (coalesced loads), and the faces
+        // take their viscous fluxes
+        if (face)
+            face_phase<DIR, NS, QT, CT, PART, MIXD, 1, true>(A, S, lane, G, A.Ti + 2 * A.np + gl,
+                                                             DIR == 1 ? A.sy : A.sz);
+        __syncthreads();
+        {
+            const int cx = tid % COLS, l = tid / COLS;
+            CT *Sc = base + cx * STRIDE;
+#pragma unroll
+            for (int m = 0; m < 10; ++m)
+                Sc[(SL::MET + m) * 32 + l] =
+                    A.metq ? CT(__ldg(A.metq + m * A.np + gA)) : ldg<CT>(A.met[m], gA);
+        }
+        __syncthreads();
+        if (face)
+            face_phase<DIR, NS, QT, CT, PART, MIXD, 2, true>(A, S, lane, G, A.Ti + 2 * A.np + gl,
+                                                             DIR == 1 ? A.sy : A.sz);
+    } else if (face) {
         face_phase<DIR, NS, QT, CT, PART, MIXD>(A, S, lane, G, A.Ti + 2 * A.np + gl,
-                                          DIR == 1 ? A.sy : A.sz);
+                                                DIR == 1 ? A.sy : A.sz);
     }
     __syncwarp();
     if (face) {
@@ -772,6 +817,16 @@ __device__ __forceinline__ void staged_block(const Args<QT> &A, int block, unsig
 template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
 __global__ void __launch_bounds__(Staged<NS, CT, PART, MIXD>::COLS * 32)
     k_pencil_staged(const __grid_constant__ Args<QT> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    staged_block<DIR, PASS, NS, QT, CT, PART, MIXD>(A, blockIdx.x, smem_raw);
+}
+
+// The same sweep held to the registers of three blocks per SM (Staged::MINB == 3).  A separate
+// kernel: naming a minimum of one block per SM changes the compiler's register choices against
+// leaving it out, so the other instances keep the plain bound above.
+template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, bool MIXD = false>
+__global__ void __launch_bounds__(Staged<NS, CT, PART, MIXD>::COLS * 32, 3)
+    k_pencil_staged3(const __grid_constant__ Args<QT> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     staged_block<DIR, PASS, NS, QT, CT, PART, MIXD>(A, blockIdx.x, smem_raw);
 }
@@ -968,12 +1023,17 @@ int launch_staged(const Args<QT> &A, cudaStream_t s) {
     using ST = Staged<NS, CT, PART, MIXD>;
     constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
     static bool done[64] = {};
-    if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD>, sm, done)) return e;
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
     const long long blocks = (long long)((A.nx + ST::COLS - 1) / ST::COLS) *
                              ((n_along + OWN - 1) / OWN) * n_c2;
-    k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    if constexpr (ST::MINB == 3) {
+        if (int e = set_smem(k_pencil_staged3<DIR, PASS, NS, QT, CT, PART, MIXD>, sm, done)) return e;
+        k_pencil_staged3<DIR, PASS, NS, QT, CT, PART, MIXD><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    } else {
+        if (int e = set_smem(k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD>, sm, done)) return e;
+        k_pencil_staged<DIR, PASS, NS, QT, CT, PART, MIXD><<<(unsigned)blocks, ST::COLS * 32, sm, s>>>(A);
+    }
     return flame_check_launch("flame_rk_stage (pencil)");
 }
 
