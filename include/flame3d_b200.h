@@ -37,7 +37,12 @@ extern "C" {
 typedef struct CUstream_st *flame_stream_t; /* identical to cudaStream_t */
 
 #define FLAME_NG 4      /* ghost layers; parse_mesh.jl:5 */
-#define FLAME_MAX_NS 16 /* largest species count compiled in */
+/* Largest species count: every 1:1 entry point and the fills take 1..FLAME_MAX_NS species; the
+ * fused stage (flame_rk_stage*, flame_transport, flame_rk_stage_noalloc) and the batches are
+ * compiled for 1..FLAME_FUSED_MAX_NS and return FLAME_EUNSUPPORTED above (the reference's CH4
+ * mechanism, 21 species, runs on the 1:1 path only once FLAME_MAX_NS is raised). */
+#define FLAME_MAX_NS 16
+#define FLAME_FUSED_MAX_NS 9
 
 enum {
     FLAME_OK = 0,

@@ -163,3 +163,24 @@ def test_fill_ib_averages_and_mirrors(f3d, oracle):
         assert q[6] == pytest.approx(e, rel=1e-13)
     keep = tag.ravel() != 3
     assert np.array_equal(Q.reshape(7, -1)[:, keep], Qf[:, keep])  # only ghost points change
+
+
+def test_inflow_case_has_reference_boundaries_and_all_branches(f3d, oracle):
+    """cases.inflow_jet on the oracle: the reference's fills put the inflow state on the x-low
+    planes (boundary.jl:9-41), and the sensor spans all three hybrid branches (schemes.jl:86-437:
+    UP7 below 1e-3, WENO-Z below 0.1, minmod above), so the GPU parity test on this case
+    exercises every branch next to the non-periodic boundaries."""
+    import ctypes as C
+    import numpy as np
+    case = f3d.inflow_jet(nx=32, ny=16, nz=16, ns=5)
+    oc = oracle.OracleCase(case)
+    ng = 4
+    assert np.allclose(oc.Q[1, :, :, :ng + 1], 1000.0)
+    assert np.allclose(oc.Q[5, :, :, :ng + 1], 270.65)
+    phi = np.zeros(oc.Q.shape[1:])
+    oracle.load().oracle_shockSensor(C.byref(oc.grid), oracle.ptr(phi), oracle.ptr(oc.Q))
+    inner = oracle.interior(phi)
+    assert (inner < 1e-3).any() and ((inner >= 1e-3) & (inner < 0.1)).any() and (inner >= 0.1).any()
+    oc.step()
+    assert np.isfinite(oc.U).all()
+

@@ -44,18 +44,6 @@ def case(f3d):
     return f3d.inflow_jet(nx=32, ny=16, nz=16, ns=5)
 
 
-def test_case_has_reference_boundaries_and_all_branches(f3d, oracle, case):
-    """The fills put the inflow state on the x-low planes, and the sensor spans all three
-    hybrid branches (schemes.jl:86-437: UP7 below 1e-3, WENO-Z below 0.1, minmod above)."""
-    oc = oracle.OracleCase(case)
-    ng = 4
-    assert np.allclose(oc.Q[1, :, :, :ng + 1], 1000.0) and np.allclose(oc.Q[5, :, :, :ng + 1], 270.65)
-    phi = np.zeros(oc.Q.shape[1:])
-    oracle.load().oracle_shockSensor(C.byref(oc.grid), oracle.ptr(phi), oracle.ptr(oc.Q))
-    inner = oracle.interior(phi)
-    assert (inner < 1e-3).any() and ((inner >= 1e-3) & (inner < 0.1)).any() and (inner >= 0.1).any()
-
-
 def test_sequence_matches_oracle(f3d, oracle, cuda_ok, case):
     dc = f3d.solver_module().DeviceCase(case, sequence_buffers=True)
     oc = oracle.OracleCase(case)
