@@ -142,6 +142,11 @@ __device__ __forceinline__ void prep_block(const Args<QT> &A, int bid) {
     if (c >= A.np) return;
     const int gx = c % A.tx, gy = (c / A.tx) % A.ty, gz = c / A.sz;
     const QT *P = A.Qi + 4 * A.np;
+    // the inputs of Y before any store (a later load could not pass a store it may alias)
+    const double rinv = 1 / jmax(double(A.Qi[c]), kEps);
+    double ri[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) ri[n] = A.ri[c + n * A.np];
     double phi = 0;
     if (gx > 0 && gx < A.tx - 1 && gy > 0 && gy < A.ty - 1 && gz > 0 && gz < A.tz - 1) {
         // schemes.jl:10-22 in the arithmetic type of Q with exact divisions, so the branch
@@ -157,9 +162,8 @@ __device__ __forceinline__ void prep_block(const Args<QT> &A, int bid) {
         phi = phx + phy + phz;
     }
     A.aux[c] = QT(phi);
-    const double rinv = 1 / jmax(double(A.Qi[c]), kEps);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) A.aux[c + (1 + n) * A.np] = QT(jmax(A.ri[c + n * A.np] * rinv, 0.0));
+    for (int n = 0; n < NS; ++n) A.aux[c + (1 + n) * A.np] = QT(jmax(ri[n] * rinv, 0.0));
 }
 
 template <int NS, typename QT>
@@ -474,22 +478,35 @@ __device__ __forceinline__ void finish_cell(const Args<QT> &A, int g, int gx, in
                                             const MixTables<NS, QT> *mt = nullptr) {
     const int np = A.np;
     const double Jact = A.met[9][g] * A.dt;
+    // every input first: the stores below could alias them as far as the compiler knows, so
+    // loads placed after a store would each wait for the one before
+    double u0[5], r0[NS], un0[5], rn0[NS];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) u0[n] = A.U[g + n * np];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) r0[n] = A.ri[g + n * np];
+    if (A.stage > 1) {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) un0[n] = A.Un[g + n * np];
+#pragma unroll
+        for (int n = 0; n < NS; ++n) rn0[n] = A.rn[g + n * np];
+    }
+    // the RK3 update, utils.jl:95-112 (the multiply-adds spelled out, so that every kernel
+    // that inlines this rounds them alike)
     double Uc[5], r[NS];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-        const double u0 = A.U[g + n * np];
-        if (A.stage == 1) A.Un[g + n * np] = u0;
-        double un = u0 + rhs[n] * Jact;
-        if (A.stage > 1) un = un * A.ca + A.Un[g + n * np] * A.cb;
+        if (A.stage == 1) A.Un[g + n * np] = u0[n];
+        double un = fma(rhs[n], Jact, u0[n]);
+        if (A.stage > 1) un = fma(un, A.ca, un0[n] * A.cb);
         Uc[n] = un;
         A.U[g + n * np] = un;
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        const double r0 = A.ri[g + n * np];
-        if (A.stage == 1) A.rn[g + n * np] = r0;
-        double rv = r0 + rhs[5 + n] * Jact;
-        if (A.stage > 1) rv = rv * A.ca + A.rn[g + n * np] * A.cb;
+        if (A.stage == 1) A.rn[g + n * np] = r0[n];
+        double rv = fma(rhs[5 + n], Jact, r0[n]);
+        if (A.stage > 1) rv = fma(rv, A.ca, rn0[n] * A.cb);
         r[n] = rv;
     }
     // c2Prim, utils.jl:2-48
