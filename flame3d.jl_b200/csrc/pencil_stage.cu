@@ -899,11 +899,14 @@ struct BatchShape {
     static constexpr int XW = Wpb<0>::value;  // pencils of an x item (its warps)
     static constexpr size_t SMEM = sizeof(CT) * ST::STRIDE * ST::COLS;
     static constexpr size_t SMEM_X = smem_bytes<NS, CT, XW>();
-    // x blocks per SM that the shared memory allows (228 KB, 1 KB reserved per block), as the
-    // register bound that lets them all be resident; in FP32, whose blocks are small, at most
-    // six (80 registers) up to three species and four (128) above, where fewer would spill
+    // x blocks per SM, as the register bound: what the shared memory allows (228 KB, 1 KB
+    // reserved per block), but at most what the stand-alone x sweep's own register count gives
+    // at this species count and precision (its item loop and indexed descriptors cost the
+    // persistent kernel registers: unbounded it takes more and fits fewer blocks, bounded
+    // tighter it spills; measured on single cases and the 64-case ensemble)
     static constexpr int FIT_X = int((228 * 1024) / (SMEM_X + 1024));
-    static constexpr int CAP_X = sizeof(CT) == 8 ? 8 : (NS <= 3 ? 6 : 4);
+    static constexpr int CAP_X = sizeof(CT) == 8 ? (NS <= 1 ? 5 : NS == 2 ? 4 : NS <= 5 ? 3 : 2)
+                                                 : (NS <= 1 ? 7 : NS <= 3 ? 5 : NS <= 7 ? 4 : 3);
     static constexpr int MINB_X = FIT_X < 1 ? 1 : (FIT_X > CAP_X ? CAP_X : FIT_X);
 };
 
