@@ -4,8 +4,9 @@ A `Batch` groups `DeviceCase`s that use the pencil configuration (each owns its 
 and scratch).  Two modes:
 
 * "persistent": flame_batch_* in the C ABI; one stage is two persistent launches per chunk
-  of up to 20 cases of one species count, over a (case, block) work list of every phase of
-  every case (device counters order a case's phases; `status()` reports a wait that ran out);
+  of up to 20 cases of one species count and transport family (four for the mixture-averaged
+  law 2), over a (case, block) work list of every phase of every case (device counters order a
+  case's prep before its sweeps; `status()` reports a wait that ran out);
 * "graph": every case's own launch chain (prep, z, y, x sweeps per stage) on one of several
   streams, forked and joined inside one CUDA graph, so the chains of small cases run side by
   side on the GPU and every kernel keeps its parameters in the constant bank.

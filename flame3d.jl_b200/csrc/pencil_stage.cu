@@ -656,8 +656,9 @@ __global__ void __launch_bounds__(Wpb<0>::value * 32) k_pencil_x(const __grid_co
 // The stage's finish for configuration 4: one thread per interior cell, x fastest, with the
 // complete right-hand side already in R (the x sweep summed it).
 template <int NS, typename QT, bool LAW2>
-__device__ __forceinline__ void finish_thread(const Args<QT> &A, const MixTables<NS, QT> *mt) {
-    const int c = blockIdx.x * 128 + threadIdx.x;
+__device__ __forceinline__ void finish_thread(const Args<QT> &A, const MixTables<NS, QT> *mt,
+                                              int block) {
+    const int c = block * 128 + threadIdx.x;
     if (c >= A.nx * A.ny * A.nz) return;
     const int x = c % A.nx, y = (c / A.nx) % A.ny, z = c / (A.nx * A.ny);
     const int gx = x + A.ng, gy = y + A.ng, gz = z + A.ng;
@@ -670,7 +671,7 @@ __device__ __forceinline__ void finish_thread(const Args<QT> &A, const MixTables
 
 template <int NS, typename QT>
 __global__ void __launch_bounds__(128) k_finish(const __grid_constant__ Args<QT> A) {
-    finish_thread<NS, QT, false>(A, nullptr);
+    finish_thread<NS, QT, false>(A, nullptr, blockIdx.x);
 }
 
 // The finish with the mixture-averaged law (law 2).  Its mixture rule needs up to 166 registers
@@ -681,7 +682,7 @@ __global__ void __launch_bounds__(128, 4) k_finish_mix(const __grid_constant__ A
     __shared__ MixTables<NS, QT> mt;
     mix_tables_fill<NS, QT>(A.th, A.tr, mt);
     __syncthreads();
-    finish_thread<NS, QT, true>(A, &mt);
+    finish_thread<NS, QT, true>(A, &mt, blockIdx.x);
 }
 
 // Columns per block of the staged y / z sweeps.  Single precision: 16 consecutive x columns, so
@@ -849,28 +850,33 @@ __global__ void __launch_bounds__(Staged<NS, CT, PART, MIXD>::COLS * 32, 3)
 }
 
 // ---------------------------------------------------------------------- batched, persistent
-// Two persistent launches per chunk of cases (one species count, configuration 3) and stage.
-// A work list holds, in this order, the prep blocks, z-sweep blocks and y-sweep blocks of all
-// the chunk's cases, then their x-sweep blocks (which finish the stage); item -> (case, block)
-// comes from a precomputed table.  k_batch_sweeps takes the first three phases' items in list
-// order from an atomic counter, so an item only ever waits for items taken before it: a case's
-// sweep item waits until the case's prep items are done (a counter in device memory; every wait
-// bounded: on timeout the batch's error word is set, the item is skipped and every later wait
-// gives up at once; flame_batch_status reports FLAME_ETIMEOUT).  k_batch_x follows on the
-// stream, so the stream orders the x items after every sweep item, and each kernel keeps the
-// registers of its own phases.  Cases never read each other's data, so a case's result does
-// not depend on which other cases share the batch.
+// Persistent launches per chunk of cases (one species count and transport family) and stage,
+// over a work list of (case, block) items in phase order.  Laws 0 and 1 (configuration 3's
+// shape), two launches: k_batch_sweeps<V = 0> takes the prep, z-sweep and y-sweep blocks of all
+// the chunk's cases, k_batch_x<false> the x-sweep blocks, which finish the stage.  Law 2
+// (configuration 6's shape, per-species D_k), four: k_batch_sweeps<V = 1> the prep blocks and
+// the flow-only (ns = 0) z and y sweeps, k_batch_sweeps<V = 2> the species z and y sweeps
+// (which add the enthalpy-diffusion term to the flow sweeps' energy field), k_batch_x<true> the
+// x sweeps without the finish, k_batch_finish the finishing blocks with the mixture rule.
+// Each launch takes its items in list order from its own atomic counter, so an item only ever
+// waits for items taken before it: a case's sweep item waits until the case's prep items are
+// done (a counter in device memory; every wait bounded: on timeout the batch's error word is
+// set, the item is skipped and every later wait gives up at once; flame_batch_status reports
+// FLAME_ETIMEOUT).  Every other order is the stream's: each launch follows the one before, so
+// each kernel keeps the registers of its own phases.  Cases never read each other's data, so a
+// case's result does not depend on which other cases share the batch.
 struct BatchItem {
     int c, b;  // case (index within the chunk), block within the case's phase
 };
 
 struct BatchLaunch {
     const BatchItem *items;  // work list
-    const int4 *need;        // per case: prep, z, y, x items
-    int *next;               // item counters of the two kernels (zeroed before the launches)
-    int *done;               // per case: completed prep items (zeroed before the launch)
+    const int4 *need;        // per case: prep items (x)
+    int *next;               // this launch's item counter (zeroed before the chunk's launches)
+    int *done;               // per case: completed prep items (zeroed before the launches)
     int *err;                // the batch's error word (FLAME_ETIMEOUT)
-    int p1, p2, p3, total;   // first z item, first y item, first x item, item count
+    int lo, hi;              // this launch's items: list positions [lo, hi)
+    int p1, p2;              // sweep launches: first item of the second and of the third phase
     int stall;               // test hook: case 0 waits for one prep item more than exists
 };
 
@@ -891,9 +897,14 @@ __device__ __forceinline__ bool wait_count(const int *count, int target, int *er
     return false;
 }
 
-template <int NS, typename QT, typename CT>
+// The staged sweep of a sweeps launch: V 0 the whole sweep, V 1 the flow-only sweep (the ns = 0
+// instance), V 2 the species sweep with per-species D_k.
+template <int NS, typename CT, int V>
+using SweepOf = Staged<V == 1 ? 0 : NS, CT, V == 2 ? 2 : 0, V == 2>;
+
+template <int NS, typename QT, typename CT, int V = 0>
 struct BatchShape {
-    using ST = Staged<NS, CT>;
+    using ST = SweepOf<NS, CT, V>;
     static constexpr int COLS = ST::COLS;
     static constexpr int NT = ST::COLS * 32;  // threads of a sweep block (prep, z, y items)
     static constexpr int XW = Wpb<0>::value;  // pencils of an x item (its warps)
@@ -926,26 +937,30 @@ __device__ __forceinline__ const Args<QT> &batch_args(int c) {
     return reinterpret_cast<const Args<QT> *>(c_batch_args)[c];
 }
 
-// Prep, z-sweep and y-sweep items (list positions [0, L.p3)): a sweep item first waits until
-// its case's prep items are done.  Thread 0 takes the next item from the counter while the
-// block works on the current one.
-template <int NS, typename QT, typename CT>
-__global__ void __launch_bounds__(BatchShape<NS, QT, CT>::NT)
+// Sweep items (list positions [L.lo, L.hi)): prep items up to L.p1, then z-sweep items up to
+// L.p2, then y-sweep items.  A sweep item first waits until its case's prep items are done (in
+// the species launch, V 2, which has no prep items, the prep launch before it has done them
+// all and the wait ends at its first look).  Thread 0 takes the next item from the counter
+// while the block works on the current one.
+template <int NS, typename QT, typename CT, int V>
+__global__ void __launch_bounds__(BatchShape<NS, QT, CT, V>::NT)
     k_batch_sweeps(const __grid_constant__ BatchLaunch L) {
-    using BS = BatchShape<NS, QT, CT>;
+    using BS = BatchShape<NS, QT, CT, V>;
+    constexpr int SN = V == 1 ? 0 : NS;               // the species the sweeps carry
+    constexpr int PART = V == 2 ? 2 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_next, s_ok;
-    if (threadIdx.x == 0) s_next = atomicAdd(L.next, 1);
+    if (threadIdx.x == 0) s_next = L.lo + atomicAdd(L.next, 1);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = s_next;
         __syncthreads();
         const int item = s_item;
-        if (item >= L.p3) return;
+        if (item >= L.hi) return;
         const BatchItem it = L.items[item];
         const int ph = item < L.p1 ? 0 : item < L.p2 ? 1 : 2;
         if (threadIdx.x == 0) {
-            s_next = atomicAdd(L.next, 1);  // in flight while the item runs
+            s_next = L.lo + atomicAdd(L.next, 1);  // in flight while the item runs
             s_ok = ph == 0 || wait_count(L.done + 4 * it.c,
                                          L.need[it.c].x + (L.stall && it.c == 0), L.err);
         }
@@ -953,13 +968,15 @@ __global__ void __launch_bounds__(BatchShape<NS, QT, CT>::NT)
         const Args<QT> &A = batch_args<QT>(it.c);
         if (s_ok) {
             if (ph == 0) {
+                if constexpr (V != 2) {
 #pragma unroll
-                for (int k = 0; k < kPrepPerThread; ++k)
-                    prep_block<NS, QT, BS::NT>(A, it.b * kPrepPerThread + k);
+                    for (int k = 0; k < kPrepPerThread; ++k)
+                        prep_block<NS, QT, BS::NT>(A, it.b * kPrepPerThread + k);
+                }
             } else if (ph == 1) {
-                staged_block<2, 0, NS, QT, CT>(A, it.b, smem_raw);
+                staged_block<2, 0, SN, QT, CT, PART, V == 2>(A, it.b, smem_raw);
             } else {
-                staged_block<1, 1, NS, QT, CT>(A, it.b, smem_raw);
+                staged_block<1, 1, SN, QT, CT, PART, V == 2>(A, it.b, smem_raw);
             }
         }
         __syncthreads();  // the item's writes are done and its shared memory is free
@@ -970,26 +987,53 @@ __global__ void __launch_bounds__(BatchShape<NS, QT, CT>::NT)
     }
 }
 
-// x-sweep items (list positions [L.p3, L.total)), launched after k_batch_sweeps on the same
-// stream, so all of every case's z and y items are done: they finish the stage.  They take
-// items from a second counter (L.next[1]), in the same way.
-template <int NS, typename QT, typename CT>
+// x-sweep items (list positions [L.lo, L.hi)), launched after the sweeps on the same stream, so
+// all of every case's z and y items are done.  MIX (law 2): the x sweep with per-species D_k,
+// which leaves the finish to k_batch_finish; otherwise the x sweep finishes the stage.
+template <int NS, typename QT, typename CT, bool MIX>
 __global__ void __launch_bounds__(BatchShape<NS, QT, CT>::XW * 32, BatchShape<NS, QT, CT>::MINB_X)
     k_batch_x(const __grid_constant__ BatchLaunch L) {
     using BS = BatchShape<NS, QT, CT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_next;
-    if (threadIdx.x == 0) s_next = L.p3 + atomicAdd(L.next + 1, 1);
+    if (threadIdx.x == 0) s_next = L.lo + atomicAdd(L.next, 1);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = s_next;
         __syncthreads();
         const int item = s_item;
-        if (item >= L.total) return;
+        if (item >= L.hi) return;
         const BatchItem it = L.items[item];
-        if (threadIdx.x == 0) s_next = L.p3 + atomicAdd(L.next + 1, 1);
+        if (threadIdx.x == 0) s_next = L.lo + atomicAdd(L.next, 1);
         if (!*(volatile const int *)L.err)
-            x_block<NS, QT, CT, true, false, BS::XW>(batch_args<QT>(it.c), it.b, smem_raw);
+            x_block<NS, QT, CT, !MIX, MIX, BS::XW>(batch_args<QT>(it.c), it.b, smem_raw);
+    }
+}
+
+// Finishing items of law 2 (list positions [L.lo, L.hi)), after the x items: 128 cells each,
+// with the mixture rule's tables of the item's case in shared memory (filled again when the
+// block moves on to another case; items come in case order, so that is rare).
+template <int NS, typename QT>
+__global__ void __launch_bounds__(128, 4) k_batch_finish(const __grid_constant__ BatchLaunch L) {
+    __shared__ MixTables<NS, QT> mt;
+    __shared__ int s_item, s_next;
+    int filled = -1;  // the case whose tables mt holds
+    if (threadIdx.x == 0) s_next = L.lo + atomicAdd(L.next, 1);
+    for (;;) {
+        __syncthreads();  // also: every thread is done with mt before it is filled again
+        if (threadIdx.x == 0) s_item = s_next;
+        __syncthreads();
+        const int item = s_item;
+        if (item >= L.hi) return;
+        const BatchItem it = L.items[item];
+        if (threadIdx.x == 0) s_next = L.lo + atomicAdd(L.next, 1);
+        const Args<QT> &A = batch_args<QT>(it.c);
+        if (it.c != filled) {  // block-uniform
+            mix_tables_fill<NS, QT>(A.th, A.tr, mt);
+            __syncthreads();
+            filled = it.c;
+        }
+        if (!*(volatile const int *)L.err) finish_thread<NS, QT, true>(A, &mt, it.b);
     }
 }
 
@@ -1150,25 +1194,39 @@ extern "C" size_t flame_stage_scratch_bytes(const FlameGrid *g, int precision) {
 
 // ============================================================================= batches
 // A batch advances many independent cases per stage: the cases are grouped by species count and
-// the groups cut into chunks of at most kConstCases cases; per chunk and stage a copy of the
-// chunk's descriptors into the constant table, a memset of its counters and two persistent
-// launches, k_batch_sweeps (prep, z, y items) and k_batch_x (the finishing x items).
+// transport family (laws 0 and 1, or law 2) and the groups cut into chunks of at most
+// kConstCases cases; per chunk and stage a copy of the chunk's descriptors into the constant
+// table, a memset of its counters and its persistent launches (two, or four for law 2).
 // Descriptors for the three stages and both in/out parities, the work lists and the per-case
 // item counts are uploaded once, into device workspace the caller owns, so flame_batch_stage
 // issues copies, memsets and launches only (capturable as a CUDA graph).
 #include <algorithm>
+#include <array>
 
 namespace flame {
 namespace pencil {
 
+constexpr int kMaxPhases = 7;
+
+// The work-list shape of a chunk: its phases and the block sizes their item counts follow.
+struct BatchDims {
+    int phases = 4;  // 4 (prep, z, y, x) or, law 2, 7 (prep, flow z, flow y, species z,
+                     // species y, x, finish)
+    int nt = 0;      // threads of a prep item (those of the first sweeps launch's blocks)
+    int cols = 0;    // staged columns of the first sweeps launch's blocks
+    int cols_s = 0;  // law 2: staged columns of the species sweeps' blocks
+};
+
 struct BatchChunk {
     int ns = 0, n = 0;
+    bool mix = false;            // law 2
     const void *args[6] = {};    // device Args arrays of the chunk, index (stage - 1) * 2 + parity
     const BatchItem *items = nullptr;
-    const int4 *need = nullptr;  // per case: prep, z, y, x items
-    int *counters = nullptr;     // item counters (ints 0, 1) and per case done[4], from int 4 on
-    int p1 = 0, p2 = 0, p3 = 0, total = 0;
-    int grid = 1, grid_x = 1;    // persistent blocks of the two kernels
+    const int4 *need = nullptr;  // per case: prep items (x)
+    int *counters = nullptr;     // item counters (ints 0-3, one per launch), per case done[4]
+                                 // from int 4 on
+    int bound[kMaxPhases + 1] = {};  // first item of each phase; bound[phases] = item count
+    int grid[4] = {1, 1, 1, 1};      // persistent blocks of the launches
 };
 
 }  // namespace pencil
@@ -1189,48 +1247,78 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 template <typename QT>
 size_t args_size() { return sizeof(Args<QT>); }
 
-// Items of one case in each phase (prep, z, y, x), for a chunk whose sweep blocks have `nt`
-// threads and `cols` staged columns, and whose x items hold `xw` pencils.
-inline void case_items(const FlameGrid &g, int cols, int nt, int xw, int items[4]) {
+// Items of one case in each phase of a chunk of shape d.
+inline void case_items(const FlameGrid &g, const BatchDims &d, int items[kMaxPhases]) {
     const long long tx = g.nx + 2LL * g.ng, ty = g.ny + 2LL * g.ng, tz = g.nz + 2LL * g.ng;
     const long long np = tx * ty * tz;
-    const int nxb = (g.nx + cols - 1) / cols;
-    items[0] = (int)((np + (long long)nt * kPrepPerThread - 1) / ((long long)nt * kPrepPerThread));
-    items[1] = nxb * ((g.nz + OWN - 1) / OWN) * g.ny;  // z sweep
-    items[2] = nxb * ((g.ny + OWN - 1) / OWN) * g.nz;  // y sweep
+    auto zsweep = [&](int cols) { return ((g.nx + cols - 1) / cols) * ((g.nz + OWN - 1) / OWN) * g.ny; };
+    auto ysweep = [&](int cols) { return ((g.nx + cols - 1) / cols) * ((g.ny + OWN - 1) / OWN) * g.nz; };
+    const long long per = (long long)d.nt * kPrepPerThread;
+    items[0] = (int)((np + per - 1) / per);
+    items[1] = zsweep(d.cols);
+    items[2] = ysweep(d.cols);
+    int k = 3;
+    if (d.phases == 7) items[3] = zsweep(d.cols_s), items[4] = ysweep(d.cols_s), k = 5;
     const long long warps = (long long)g.ny * g.nz * ((g.nx + OWN - 1) / OWN);
-    items[3] = (int)((warps + xw - 1) / xw);
+    items[k] = (int)((warps + Wpb<0>::value - 1) / Wpb<0>::value);
+    if (d.phases == 7) items[6] = (int)(((long long)g.nx * g.ny * g.nz + 127) / 128);
 }
 
 template <int NS, typename QT, typename CT>
-void batch_shape(int &cols, int &nt) {
-    cols = BatchShape<NS, QT, CT>::COLS;
-    nt = BatchShape<NS, QT, CT>::NT;
+BatchDims batch_dims(bool mix) {
+    BatchDims d;
+    if (mix) {
+        d.phases = 7;
+        d.nt = BatchShape<NS, QT, CT, 1>::NT;
+        d.cols = BatchShape<NS, QT, CT, 1>::COLS;
+        d.cols_s = BatchShape<NS, QT, CT, 2>::COLS;
+    } else {
+        d.nt = BatchShape<NS, QT, CT>::NT;
+        d.cols = BatchShape<NS, QT, CT>::COLS;
+    }
+    return d;
+}
+
+// Blocks of a persistent launch: as many as fit on the device at once, at most one per item.
+template <typename K>
+int persistent_grid(K kernel, int threads, size_t smem, bool *done, int items, int &grid) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (smem)
+        if (int e = set_smem(kernel, smem, done)) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
+    grid = std::max(1, std::min(items, sms * std::max(occ, 1)));
+    return FLAME_OK;
 }
 
 template <int NS, typename QT, typename CT>
 int batch_grid(BatchChunk &bc) {
-    using BS = BatchShape<NS, QT, CT>;
-    int dev = 0, sms = 0, occ = 0, occx = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    static bool d0[64] = {}, d1[64] = {};
-    if (int e = set_smem(k_batch_sweeps<NS, QT, CT>, BS::SMEM, d0)) return e;
-    if (int e = set_smem(k_batch_x<NS, QT, CT>, BS::SMEM_X, d1)) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_sweeps<NS, QT, CT>, BS::NT,
-                                                  BS::SMEM);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occx, k_batch_x<NS, QT, CT>, BS::XW * 32,
-                                                  BS::SMEM_X);
-    const int cap = sms * (occ > 0 ? occ : 1), capx = sms * (occx > 0 ? occx : 1);
-    bc.grid = std::max(1, std::min(bc.p3, cap));
-    bc.grid_x = std::max(1, std::min(bc.total - bc.p3, capx));
+    using B0 = BatchShape<NS, QT, CT>;
+    using B1 = BatchShape<NS, QT, CT, 1>;
+    using B2 = BatchShape<NS, QT, CT, 2>;
+    static bool d[5][64] = {};
+    const int *b = bc.bound;
+    int e = FLAME_OK;
+    if (!bc.mix) {
+        if (!e) e = persistent_grid(k_batch_sweeps<NS, QT, CT, 0>, B0::NT, B0::SMEM, d[0], b[3] - b[0], bc.grid[0]);
+        if (!e) e = persistent_grid(k_batch_x<NS, QT, CT, false>, B0::XW * 32, B0::SMEM_X, d[1], b[4] - b[3], bc.grid[1]);
+    } else {
+        if (!e) e = persistent_grid(k_batch_sweeps<NS, QT, CT, 1>, B1::NT, B1::SMEM, d[2], b[3] - b[0], bc.grid[0]);
+        if (!e) e = persistent_grid(k_batch_sweeps<NS, QT, CT, 2>, B2::NT, B2::SMEM, d[3], b[5] - b[3], bc.grid[1]);
+        if (!e) e = persistent_grid(k_batch_x<NS, QT, CT, true>, B0::XW * 32, B0::SMEM_X, d[4], b[6] - b[5], bc.grid[2]);
+        if (!e) e = persistent_grid(k_batch_finish<NS, QT>, 128, 0, nullptr, b[7] - b[6], bc.grid[3]);
+    }
+    if (e) return e;
     return flame_check_launch("flame_batch_create");
 }
 
 template <int NS, typename QT, typename CT>
 int batch_launch(const BatchChunk &bc, cudaStream_t s, int stage, int parity, int *err,
                  int stall) {
-    using BS = BatchShape<NS, QT, CT>;
+    using B0 = BatchShape<NS, QT, CT>;
+    using B1 = BatchShape<NS, QT, CT, 1>;
+    using B2 = BatchShape<NS, QT, CT, 2>;
     cudaError_t ce = cudaMemcpyToSymbolAsync(c_batch_args, bc.args[(stage - 1) * 2 + parity],
                                              sizeof(Args<QT>) * (size_t)bc.n, 0,
                                              cudaMemcpyDeviceToDevice, s);
@@ -1241,25 +1329,45 @@ int batch_launch(const BatchChunk &bc, cudaStream_t s, int stage, int parity, in
     BatchLaunch L;
     L.items = bc.items;
     L.need = bc.need;
-    L.next = bc.counters;
     L.done = bc.counters + 4;
     L.err = err;
-    L.p1 = bc.p1, L.p2 = bc.p2, L.p3 = bc.p3, L.total = bc.total;
     L.stall = stall;
-    k_batch_sweeps<NS, QT, CT><<<bc.grid, BS::NT, BS::SMEM, s>>>(L);
+    // launch k: its counter, items [lo, hi) and, for the sweeps, the starts of phases 1 and 2
+    auto set = [&](int k, int lo, int hi, int p1, int p2) {
+        L.next = bc.counters + k;
+        L.lo = lo, L.hi = hi, L.p1 = p1, L.p2 = p2;
+    };
+    const int *b = bc.bound;
+    if (!bc.mix) {
+        set(0, b[0], b[3], b[1], b[2]);
+        k_batch_sweeps<NS, QT, CT, 0><<<bc.grid[0], B0::NT, B0::SMEM, s>>>(L);
+        if (int e = flame_check_launch("flame_batch_stage")) return e;
+        set(1, b[3], b[4], b[4], b[4]);
+        k_batch_x<NS, QT, CT, false><<<bc.grid[1], B0::XW * 32, B0::SMEM_X, s>>>(L);
+        return flame_check_launch("flame_batch_stage");
+    }
+    set(0, b[0], b[3], b[1], b[2]);
+    k_batch_sweeps<NS, QT, CT, 1><<<bc.grid[0], B1::NT, B1::SMEM, s>>>(L);
     if (int e = flame_check_launch("flame_batch_stage")) return e;
-    k_batch_x<NS, QT, CT><<<bc.grid_x, BS::XW * 32, BS::SMEM_X, s>>>(L);
+    set(1, b[3], b[5], b[3], b[4]);  // no prep phase: p1 = lo
+    k_batch_sweeps<NS, QT, CT, 2><<<bc.grid[1], B2::NT, B2::SMEM, s>>>(L);
+    if (int e = flame_check_launch("flame_batch_stage")) return e;
+    set(2, b[5], b[6], b[6], b[6]);
+    k_batch_x<NS, QT, CT, true><<<bc.grid[2], B0::XW * 32, B0::SMEM_X, s>>>(L);
+    if (int e = flame_check_launch("flame_batch_stage")) return e;
+    set(3, b[6], b[7], b[7], b[7]);
+    k_batch_finish<NS, QT><<<bc.grid[3], 128, 0, s>>>(L);
     return flame_check_launch("flame_batch_stage");
 }
 
-// what: 0 the chunk's block shape (cols, nt), 1 its persistent grids, 2 a stage launch
+// what: 0 the chunk's work-list shape (*dims), 1 its persistent grids, 2 a stage launch
 template <typename QT, typename CT>
 int batch_dispatch(int what, BatchChunk &bc, cudaStream_t s, int stage, int parity, int *err,
-                   int stall, int *cols, int *nt) {
+                   int stall, BatchDims *dims) {
     switch (bc.ns) {
 #define CASE(N)                                                                   \
     case N:                                                                       \
-        if (what == 0) return batch_shape<N, QT, CT>(*cols, *nt), FLAME_OK;       \
+        if (what == 0) return *dims = batch_dims<N, QT, CT>(bc.mix), FLAME_OK;    \
         if (what == 1) return batch_grid<N, QT, CT>(bc);                          \
         return batch_launch<N, QT, CT>(bc, s, stage, parity, err, stall);
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9)
@@ -1270,11 +1378,10 @@ int batch_dispatch(int what, BatchChunk &bc, cudaStream_t s, int stage, int pari
 }
 
 inline int batch_dispatch_p(int precision, int what, BatchChunk &bc, cudaStream_t s, int stage,
-                            int parity, int *err, int stall, int *cols = nullptr,
-                            int *nt = nullptr) {
+                            int parity, int *err, int stall, BatchDims *dims = nullptr) {
     return precision == 0
-               ? batch_dispatch<double, double>(what, bc, s, stage, parity, err, stall, cols, nt)
-               : batch_dispatch<float, float>(what, bc, s, stage, parity, err, stall, cols, nt);
+               ? batch_dispatch<double, double>(what, bc, s, stage, parity, err, stall, dims)
+               : batch_dispatch<float, float>(what, bc, s, stage, parity, err, stall, dims);
 }
 
 template <typename QT>
@@ -1302,7 +1409,9 @@ namespace {
 // workspace: the batch's error word, then per chunk six descriptor arrays, the work list, the
 // per-case counts and the counters, each aligned to 256 bytes.
 struct ChunkPlan {
-    int ns = 0, cols = 0, nt = 0;
+    int ns = 0;
+    bool mix = false;  // law 2
+    flame::pencil::BatchDims dims;
     std::vector<int> members;  // case indices
     long long total = 0;
     size_t args_at[6] = {}, items_at = 0, need_at = 0, counters_at = 0;
@@ -1313,30 +1422,35 @@ struct Layout {
     size_t bytes = 0;
 };
 
+// A case's group: its species count, and whether it has per-species D_k (law 2).
+int group_of(const FlameCaseDesc &c) { return 2 * c.grid.ns + (c.transport.law == 2); }
+
 int plan_layout(const FlameCaseDesc *cases, int n, int precision, Layout &L) {
-    std::vector<int> nss;
+    std::vector<int> groups;
     for (int i = 0; i < n; ++i)
-        if (std::find(nss.begin(), nss.end(), cases[i].grid.ns) == nss.end())
-            nss.push_back(cases[i].grid.ns);
-    for (int ns : nss) {
+        if (std::find(groups.begin(), groups.end(), group_of(cases[i])) == groups.end())
+            groups.push_back(group_of(cases[i]));
+    for (int grp : groups) {
         flame::pencil::BatchChunk probe;
-        probe.ns = ns;
-        int cols = 0, nt = 0;
+        probe.ns = grp / 2, probe.mix = grp % 2;
+        flame::pencil::BatchDims dims;
         if (int e = flame::pencil::batch_dispatch_p(precision, 0, probe, nullptr, 1, 0, nullptr,
-                                                    0, &cols, &nt))
+                                                    0, &dims))
             return e;
+        bool fresh = true;
         for (int i = 0; i < n; ++i) {
-            if (cases[i].grid.ns != ns) continue;
-            if (L.chunks.empty() || L.chunks.back().ns != ns ||
-                (int)L.chunks.back().members.size() == flame::pencil::kConstCases) {
+            if (group_of(cases[i]) != grp) continue;
+            if (fresh || (int)L.chunks.back().members.size() == flame::pencil::kConstCases) {
                 L.chunks.emplace_back();
-                L.chunks.back().ns = ns, L.chunks.back().cols = cols, L.chunks.back().nt = nt;
+                L.chunks.back().ns = probe.ns, L.chunks.back().mix = probe.mix;
+                L.chunks.back().dims = dims;
+                fresh = false;
             }
             ChunkPlan &c = L.chunks.back();
             c.members.push_back(i);
-            int it[4];
-            flame::pencil::case_items(cases[i].grid, cols, nt, flame::pencil::Wpb<0>::value, it);
-            c.total += (long long)it[0] + it[1] + it[2] + it[3];
+            int it[flame::pencil::kMaxPhases] = {};
+            flame::pencil::case_items(cases[i].grid, dims, it);
+            for (int ph = 0; ph < dims.phases; ++ph) c.total += it[ph];
         }
     }
     const size_t asz = precision == 0 ? flame::pencil::args_size<double>()
@@ -1372,10 +1486,8 @@ int check_case(const FlameCaseDesc &c, int i) {
     if (!b.U || !b.Un || !b.Q_in || !b.Q_out || !b.rhoi_in || !b.rhoi_out || !b.rhon ||
         !b.trans_in || !b.trans_out || !b.scratch || !c.metrics.J || !c.metrics.dxidx)
         return flame_fail(FLAME_EINVAL, "flame_batch: case %d has a NULL buffer", i);
-    if (c.transport.law != 0 && c.transport.law != 1)
-        return flame_fail(c.transport.law == 2 ? FLAME_EUNSUPPORTED : FLAME_EINVAL,
-                          "flame_batch: case %d: transport law %d (the persistent batch takes "
-                          "laws 0 and 1; law 2 runs case by case on configurations 3-6)", i,
+    if (c.transport.law < 0 || c.transport.law > 2)
+        return flame_fail(FLAME_EINVAL, "flame_batch: case %d: transport law %d", i,
                           c.transport.law);
     return FLAME_OK;
 }
@@ -1415,13 +1527,16 @@ extern "C" int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, 
     for (const ChunkPlan &cp : L.chunks) {
         flame::pencil::BatchChunk bc;
         bc.ns = cp.ns;
+        bc.mix = cp.mix;
         bc.n = (int)cp.members.size();
+        const int phases = cp.dims.phases;
         std::vector<int4> need(bc.n);
+        std::vector<std::array<int, flame::pencil::kMaxPhases>> counts(bc.n);
         for (int j = 0; j < bc.n; ++j) {
             const FlameCaseDesc &c = cases[cp.members[j]];
-            int it[4];
-            flame::pencil::case_items(c.grid, cp.cols, cp.nt, flame::pencil::Wpb<0>::value, it);
-            need[j] = make_int4(it[0], it[1], it[2], it[3]);
+            counts[j].fill(0);
+            flame::pencil::case_items(c.grid, cp.dims, counts[j].data());
+            need[j] = make_int4(counts[j][0], 0, 0, 0);
             for (int st = 1; st <= 3; ++st)
                 for (int par = 0; par < 2; ++par) {
                     const size_t at = cp.args_at[(st - 1) * 2 + par] + asz * j;
@@ -1429,23 +1544,21 @@ extern "C" int flame_batch_create(FlameBatch **out, const FlameCaseDesc *cases, 
                     else flame::pencil::fill_args<float>(host, at, c, st, par);
                 }
         }
-        // work list: every case's prep items, then z, then y, then x items
+        // work list: phase by phase (prep, z, y, ... as BatchDims lists them), each phase's
+        // items case by case
         BatchItem *items = reinterpret_cast<BatchItem *>(host.data() + cp.items_at);
         long long w = 0;
-        int first[4] = {};
-        for (int ph = 0; ph < 4; ++ph) {
-            first[ph] = (int)w;
-            for (int j = 0; j < bc.n; ++j) {
-                const int cnt = ph == 0 ? need[j].x : ph == 1 ? need[j].y : ph == 2 ? need[j].z : need[j].w;
-                for (int b = 0; b < cnt; ++b) items[w++] = BatchItem{j, b};
-            }
+        for (int ph = 0; ph < phases; ++ph) {
+            bc.bound[ph] = (int)w;
+            for (int j = 0; j < bc.n; ++j)
+                for (int b = 0; b < counts[j][ph]; ++b) items[w++] = BatchItem{j, b};
         }
+        bc.bound[phases] = (int)w;
         memcpy(host.data() + cp.need_at, need.data(), sizeof(int4) * bc.n);
         for (int v = 0; v < 6; ++v) bc.args[v] = dev + cp.args_at[v];
         bc.items = reinterpret_cast<const BatchItem *>(dev + cp.items_at);
         bc.need = reinterpret_cast<const int4 *>(dev + cp.need_at);
         bc.counters = reinterpret_cast<int *>(dev + cp.counters_at);
-        bc.p1 = first[1], bc.p2 = first[2], bc.p3 = first[3], bc.total = (int)w;
         if (int e = flame::pencil::batch_dispatch_p(precision, 1, bc, s, 1, 0, B->err, 0)) {
             delete B;
             return e;

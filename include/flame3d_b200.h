@@ -425,14 +425,17 @@ int flame_transport_boundary(const FlameGrid *g, flame_stream_t stream, const vo
 
 /* ---------------------------------------------------------------------------------------
  * Batches (no reference counterpart): many independent periodic cases, each with its own
- * grid, species count, thermodynamics, transport (laws 0 and 1), dt and buffers, advanced
- * together by persistent kernels (configuration 3).  Cases are grouped by species count and cut
- * into chunks of at most 20; per chunk and stage the chunk's descriptors go into a constant-
- * memory table and two persistent kernels run: the first takes the prep, z-sweep and y-sweep
- * blocks of every case of the chunk in list order, a case's sweep blocks waiting on a device
- * counter for that case's prep blocks; the second, after it on the stream, runs the x-sweep
- * blocks, which finish the stage.  Every wait is bounded: when one runs out (about half a
- * second) the batch's error word is set and the remaining items are skipped;
+ * grid, species count, thermodynamics, transport (laws 0, 1 and 2), dt and buffers, advanced
+ * together by persistent kernels.  Cases are grouped by species count and transport family
+ * (laws 0 and 1, or law 2) and cut into chunks of at most 20; per chunk and stage the chunk's
+ * descriptors go into a constant-memory table and the persistent kernels run one after the
+ * other on the stream, each over its part of a (case, block) work list.  Laws 0 and 1 take
+ * configuration 3's shape, two kernels: the prep, z-sweep and y-sweep blocks of every case of
+ * the chunk in list order, a case's sweep blocks waiting on a device counter for that case's
+ * prep blocks; then the x-sweep blocks, which finish the stage.  Law 2 takes configuration 6's
+ * shape, four: prep and flow-only sweeps (with the same waits), the species sweeps, the x
+ * sweeps, and the finish with the mixture rule.  Every wait is bounded: when one runs out
+ * (about half a second) the batch's error word is set and the remaining items are skipped;
  * flame_batch_status reports it.  The constant table is one per device: persistent batches on
  * one device must not run concurrently.  Descriptors and work lists for all stages and both
  * in/out parities go once into caller-owned device workspace, so a captured CUDA graph of

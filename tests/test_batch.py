@@ -127,29 +127,77 @@ def test_graph_batch_with_mixed_configurations(f3d, cuda_ok):
     b.close()
 
 
-def test_graph_batch_with_law2_case(f3d, cuda_ok):
-    """A case with mixture-averaged transport (law 2, run as configuration 6) batched in graph
-    mode with law-1 cases ends bit for bit where it ends alone; the persistent batch, whose
-    kernels carry one D per point, refuses it with FLAME_EUNSUPPORTED."""
+def _law2(f3d, ns, seed, n=12):
+    case = f3d.random_curvilinear(n=n, ns=ns, seed=seed)
+    case.transport = f3d.cases.mixture_averaged_transport(case.thermo, seed=seed)
+    return case
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_with_law2_cases(f3d, cuda_ok, mode):
+    """Cases with mixture-averaged transport (law 2, configuration 6's shape: flow and species
+    sweeps, the x sweep, the finish with the mixture rule) batched with law-1 cases of the same
+    and other species counts: each law-2 case ends bit for bit where it ends alone in a batch
+    of its own, and (the persistent launches being other kernels than the stand-alone ones)
+    within 1e-12 of the stand-alone stage."""
     S = f3d.solver_module()
     B = f3d.batch_module()
-    cases = _mix(f3d)[:3]
-    law2 = f3d.random_curvilinear(n=12, ns=4, seed=55)
-    law2.transport = f3d.cases.mixture_averaged_transport(law2.thermo, seed=55)
-    cases.append(law2)
+    law2 = [_law2(f3d, 4, 55), _law2(f3d, 2, 56, n=10)]
+    cases = _mix(f3d)[:3] + law2 + [f3d.random_curvilinear(n=10, ns=4, seed=58)]
     batched = [S.DeviceCase(c, tile=3) for c in cases]
-    alone = S.DeviceCase(law2, tile=3)
-    b = B.Batch(batched, mode="graph")
+    solo = [S.DeviceCase(c, tile=3) for c in law2]
+    ref = [S.DeviceCase(c, tile=3) for c in law2]
+    b = B.Batch(batched, mode=mode)
     b.capture()
+    b1 = [B.Batch([dc], mode=mode) for dc in solo]
     for _ in range(2):
         b.step()
-        alone.step()
-    for a, c in zip(_state(alone), _state(batched[-1])):
-        assert np.array_equal(a, c)
+        for x in b1:
+            x.step()
+        for dc in ref:
+            dc.step()
+    b.status()
+    for k, (alone, r) in enumerate(zip(solo, ref)):
+        mixed = batched[3 + k]
+        for a, m in zip(_state(alone), _state(mixed)):
+            assert np.array_equal(a, m), (mode, law2[k].name)
+        for a, c in zip(_state(mixed), _state(r)):
+            for f in range(a.shape[0]):
+                n = np.linalg.norm(c[f].ravel())
+                assert np.linalg.norm((a[f] - c[f]).ravel()) <= 1e-12 * n, (mode, law2[k].name, f)
     b.close()
-    with pytest.raises(f3d.abi.FlameError) as e:
-        B.Batch([S.DeviceCase(law2, tile=3)], mode="persistent")
-    assert e.value.code == 5
+    for x in b1:
+        x.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("ns", [2, 5, 9])
+def test_persistent_law2_matches_oracle(f3d, oracle, cuda_ok, ns, precision):
+    """The persistent law-2 launches over two RK3 steps against the oracle: 1e-12 relative L2
+    per field (partial densities included) in FP64, 1e-5 on the conserved fields in mixed
+    precision."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    case = _law2(f3d, ns, 60 + ns)
+    dc = S.DeviceCase(case, precision=precision, tile=3)
+    b = B.Batch([dc], mode="persistent")
+    oc = oracle.OracleCase(case)
+    for _ in range(2):
+        b.step()
+        oc.step()
+    b.status()
+    I = oracle.interior
+    U = dc.conserved()
+    mom = np.linalg.norm(I(oc.U[1:4]).ravel())
+    tol = 1e-12 if precision == 0 else 1e-5
+    for n in range(5):
+        ref = I(oc.U[n])
+        scale = mom if 1 <= n <= 3 else np.linalg.norm(ref.ravel())
+        assert np.linalg.norm((I(U[n]) - ref).ravel()) / scale <= tol, (n, precision)
+    if precision == 0:
+        _, r = dc.primitives()
+        assert oracle.rel_l2(I(r), I(oc.rhoi)) <= tol
+    b.close()
 
 
 @pytest.mark.parametrize("precision", [0, 1])
