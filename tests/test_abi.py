@@ -134,3 +134,31 @@ def test_size_queries_do_not_wrap(f3d, lib):
         rc = lib.flame_rk_stage(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m),
                                 C.byref(f3d.FlameThermo()), C.byref(f3d.FlameTransport()), 0)
         assert rc == 1 and "2^31" in f3d.abi.last_error(lib), ext
+
+
+def test_batch_planning_needs_no_gpu(f3d, lib):
+    """flame_batch_workspace_bytes plans on the host: it takes transport laws 0, 1 and 2 (a
+    law-2 case adds the species-sweep and finish phases to its chunk's work list, so its plan
+    is larger than the same grid's under law 1), and refuses an unknown law, a grid that is
+    not periodic, more than nine species and a NULL buffer (size 0)."""
+    def desc(law=1, ns=2, periodic=7, n=16, buf=True):
+        d = f3d.abi.FlameCaseDesc()
+        d.grid = f3d.FlameGrid(n, n, n, 4, ns, periodic)
+        d.dt = 1e-6
+        d.buf = f3d.FlameStageBuffers(*([4096 if buf else 0] * 10))
+        d.metrics = f3d.FlameMetrics(*([4096] * 10))
+        d.transport.law = law
+        return d
+
+    def plan(*descs, precision=0):
+        arr = (f3d.abi.FlameCaseDesc * len(descs))(*descs)
+        return lib.flame_batch_workspace_bytes(arr, len(descs), precision)
+
+    for precision in (0, 1):
+        one, two = plan(desc(1), precision=precision), plan(desc(2), precision=precision)
+        assert one > 0 and two > one, (precision, one, two)
+        assert plan(desc(0), desc(2), desc(1, ns=5), precision=precision) > 0
+    assert plan(desc(3)) == 0
+    assert plan(desc(periodic=3)) == 0
+    assert plan(desc(ns=10)) == 0
+    assert plan(desc(buf=False)) == 0

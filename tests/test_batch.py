@@ -250,10 +250,11 @@ def test_persistent_batch_more_cases_than_one_chunk(f3d, cuda_ok):
 def test_persistent_wait_runs_out_and_reports(f3d, cuda_ok):
     """A completion that never comes (flame_batch_test_stall): the waits give up after their
     bound, the stage returns, flame_batch_status reports FLAME_ETIMEOUT once, and the batch and
-    the GPU stay usable; nothing faults or hangs."""
+    the GPU stay usable; nothing faults or hangs.  A law-2 case gives the batch a chunk of
+    four launches too."""
     S = f3d.solver_module()
     B = f3d.batch_module()
-    cases = _mix(f3d)[:3]
+    cases = _mix(f3d)[:3] + [_law2(f3d, 3, 61, n=10)]
     dcs = [S.DeviceCase(c, tile=3) for c in cases]
     b = B.Batch(dcs, mode="persistent")
     f3d.abi.check(b.lib, b.lib.flame_batch_test_stall(b.handle, 1))
