@@ -24,6 +24,8 @@
 //
 // All indices are 32-bit: the host checks that every array holds fewer than 2^31 elements.
 
+#include <atomic>
+
 #include "common.cuh"
 
 int flame_pencil_stage(const FlameGrid *g, cudaStream_t s, int stage, double dt,
@@ -632,16 +634,18 @@ int launch(const FlameGrid &g, cudaStream_t s, int stage, double dt, const Flame
            const FlameMetrics &m, const FlameThermo &th, const FlameTransport &tr) {
     const Args<QT> A = make_args<QT>(g, stage, dt, b, m, th, tr);
     constexpr size_t sm = smem_bytes<T, NS, CT>();
-    static bool attr_set[64] = {};  // the attribute is per function and device
+    // the attribute is per function and device; atomic, as host threads on other streams may
+    // launch the same kernel at the same time (both then set it, to the same value)
+    static std::atomic<bool> attr_set[64];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    if (dev < 0 || dev >= 64 || !attr_set[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(k_stage<T, NS, QT, CT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess)
             return flame_fail(FLAME_ELAUNCH, "flame_rk_stage: %zu B shared memory: %s", sm,
                               cudaGetErrorString(e));
-        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        if (dev >= 0 && dev < 64) attr_set[dev].store(true, std::memory_order_release);
     }
     dim3 grid((g.nx + T::TX - 1) / T::TX, (g.ny + T::TY - 1) / T::TY, (g.nz + T::TZ - 1) / T::TZ);
     k_stage<T, NS, QT, CT><<<grid, T::NT, sm, s>>>(A);

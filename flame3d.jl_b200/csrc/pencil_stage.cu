@@ -25,6 +25,7 @@
 // Template parameters as in fused_stage.cu: NS species, QT storage of Q / transport, CT
 // arithmetic type of split, reconstruction and viscous fluxes.  All indices are 32-bit.
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <type_traits>
@@ -1070,15 +1071,17 @@ Args<QT> make_args(const FlameGrid &g, int stage, double dt, const FlameStageBuf
 }
 
 template <typename K>
-int set_smem(K kernel, size_t sm, bool *done) {
+int set_smem(K kernel, size_t sm, std::atomic<bool> *done) {
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && done[dev]) return FLAME_OK;
+    // atomic flags: host threads on other streams may launch the same kernel at the same time
+    // (two that both find the flag unset both set the attribute, to the same value)
+    if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return FLAME_OK;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess)
         return flame_fail(FLAME_ELAUNCH, "pencil sweep: %zu B shared memory: %s", sm,
                           cudaGetErrorString(e));
-    if (dev >= 0 && dev < 64) done[dev] = true;
+    if (dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
     return FLAME_OK;
 }
 
@@ -1086,7 +1089,7 @@ template <int DIR, int PASS, int NS, typename QT, typename CT, int PART = 0, boo
 int launch_staged(const Args<QT> &A, cudaStream_t s) {
     using ST = Staged<NS, CT, PART, MIXD>;
     constexpr size_t sm = sizeof(CT) * ST::STRIDE * ST::COLS;
-    static bool done[64] = {};
+    static std::atomic<bool> done[64];
     const int n_along = DIR == 1 ? A.ny : A.nz;
     const int n_c2 = DIR == 1 ? A.nz : A.ny;
     const long long blocks = (long long)((A.nx + ST::COLS - 1) / ST::COLS) *
@@ -1105,7 +1108,7 @@ template <int NS, typename QT, typename CT, bool FIN, bool MIXD = false>
 int launch_x(const Args<QT> &A, cudaStream_t s) {
     constexpr int WPB = Wpb<0>::value;
     constexpr size_t sm = smem_bytes<NS, CT, WPB>();
-    static bool done[64] = {};
+    static std::atomic<bool> done[64];
     if (int e = set_smem(k_pencil_x<NS, QT, CT, FIN, MIXD>, sm, done)) return e;
     const long long warps = (long long)A.ny * A.nz * ((A.nx + OWN - 1) / OWN);
     k_pencil_x<NS, QT, CT, FIN, MIXD><<<(unsigned)((warps + WPB - 1) / WPB), WPB * 32, sm, s>>>(A);
@@ -1281,7 +1284,8 @@ BatchDims batch_dims(bool mix) {
 
 // Blocks of a persistent launch: as many as fit on the device at once, at most one per item.
 template <typename K>
-int persistent_grid(K kernel, int threads, size_t smem, bool *done, int items, int &grid) {
+int persistent_grid(K kernel, int threads, size_t smem, std::atomic<bool> *done, int items,
+                    int &grid) {
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1297,7 +1301,7 @@ int batch_grid(BatchChunk &bc) {
     using B0 = BatchShape<NS, QT, CT>;
     using B1 = BatchShape<NS, QT, CT, 1>;
     using B2 = BatchShape<NS, QT, CT, 2>;
-    static bool d[5][64] = {};
+    static std::atomic<bool> d[5][64];
     const int *b = bc.bound;
     int e = FLAME_OK;
     if (!bc.mix) {
