@@ -723,7 +723,10 @@ def main() -> int:
     rh = torch.from_numpy(case.rhoi).pin_memory()
     Qo = [torch.empty_like(Qh).pin_memory() for _ in range(E2E_LANES)]
     ro = [torch.empty_like(rh).pin_memory() for _ in range(E2E_LANES)]
-    e2e_steps = E2E_LANES * max(2, min(args.steps, 21) // E2E_LANES)
+    # at least ten calls per lane: the pipeline's first upload and last download (about two
+    # steps' worth of copies) are not overlapped, and over fewer calls they would weigh as a
+    # throughput loss that a continuously running caller does not have
+    e2e_steps = E2E_LANES * max(10, min(args.steps, 60) // E2E_LANES)
     for _ in range(2):
         dc.advance_from_host(Qh, rh, 1, Qo[0], ro[0])
     barrier()
