@@ -65,6 +65,10 @@ extern "C" int flame_rk_stage_noalloc(const FlameGrid *g, flame_stream_t s, int 
                                       int precision) {
     if (int e = flame_check_grid(g, "flame_rk_stage_noalloc")) return e;
     if (!b) return flame_fail(FLAME_EINVAL, "flame_rk_stage_noalloc: NULL buffers");
+    // the stage checks the rest; this one comes before the array's address lookup, so that a
+    // grid no configuration takes is refused without touching the device
+    if (g->nx < FLAME_NG || g->ny < FLAME_NG || g->nz < FLAME_NG)
+        return flame_fail(FLAME_EINVAL, "flame_rk_stage_noalloc: extents must be >= %d", FLAME_NG);
     if (precision != 0 && precision != 1)
         return flame_fail(FLAME_EINVAL, "flame_rk_stage_noalloc: precision=%d must be 0 or 1",
                           precision);

@@ -162,3 +162,21 @@ def test_batch_planning_needs_no_gpu(f3d, lib):
     assert plan(desc(periodic=3)) == 0
     assert plan(desc(ns=10)) == 0
     assert plan(desc(buf=False)) == 0
+
+
+def test_fused_stage_refuses_extents_below_the_ghost_width(f3d, lib):
+    """The fused stage (and the no-alloc entry, which runs through it) needs every extent >= 4
+    (a stencil reaches 3 cells past a face and the periodic images are single copies); smaller
+    grids are refused before any CUDA call, on every configuration."""
+    b = f3d.FlameStageBuffers(1, 2, 3, 4, 5, 6, 7, 8, 9)
+    m = f3d.FlameMetrics(*([1] * 10))
+    th, tr = f3d.FlameThermo(), f3d.FlameTransport()
+    for ext in ((3, 8, 8), (8, 1, 8), (8, 8, 2)):
+        g = f3d.FlameGrid(*ext, 4, 1, 7)
+        for tile in range(7):
+            rc = lib.flame_rk_stage_tiled(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m),
+                                          C.byref(th), C.byref(tr), 0, tile)
+            assert rc == 1 and "extents must be >= 4" in f3d.abi.last_error(lib), (ext, tile)
+        rc = lib.flame_rk_stage_noalloc(C.byref(g), None, 1, 1e-3, C.byref(b), C.byref(m),
+                                        C.byref(th), C.byref(tr), 0)
+        assert rc == 1 and "extents must be >= 4" in f3d.abi.last_error(lib), ext
