@@ -14,8 +14,9 @@
  *     which is the only value the fused entry points accept.
  *   - Every call is asynchronous on `stream` (NULL = legacy default stream) and returns
  *     FLAME_OK or an error code; flame_last_error() gives the message of the calling thread.
- *   - Global state of the library: a per-thread error string; per device, flags recording that
- *     a kernel's dynamic shared-memory limit has been raised (set once, never cleared); the
+ *   - Global state of the library: a per-thread error string; per device, atomic flags
+ *     recording that a kernel's dynamic shared-memory limit has been raised (set once, never
+ *     cleared; host threads on different streams may call concurrently); the
  *     persistent batch's constant-memory descriptor table (one per device, see flame_batch_*);
  *     and, used only by flame_rk_stage_noalloc, a library-held scratch array with its
  *     per-device address cache (described at that entry point).  No call allocates device
