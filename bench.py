@@ -613,7 +613,7 @@ def max_over_ranks(ms: float, device=None) -> float:
     GPU under NCCL, the CPU under gloo)."""
     import torch
     import torch.distributed as dist
-    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+    if not (dist.is_available() and dist.is_initialized()):
         return float(ms)
     t = torch.tensor([ms], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -673,7 +673,10 @@ def main() -> int:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
+    # under torchrun the ranks always form an NCCL group, one rank included, so that the
+    # barriers and the max-over-ranks reduction run the same calls at every N
+    distributed = "WORLD_SIZE" in os.environ
+    if distributed:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=dev)
@@ -683,7 +686,7 @@ def main() -> int:
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
-        if world > 1:
+        if distributed:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
@@ -760,7 +763,7 @@ def main() -> int:
     d2h = (Qo[0].numel() * Qo[0].element_size() + ro[0].numel() * ro[0].element_size())
 
     if rank != 0:
-        if world > 1:
+        if distributed:
             dist.destroy_process_group()
         return 0
 
@@ -791,8 +794,8 @@ def main() -> int:
                         "flop_per_cell_stage": fc["flop_per_cell_stage"],
                         "peak_source": "measured (csrc/probe/fp64_peak.cu, this run)",
                         "counts_source": counts.get("source")}
-        roof["limiter"] = ("neither roof: FP64 issue and latency at 16 of 64 warps per SM "
-                           "(profiles/fp64_counts_jet128x64x64.md)")
+        roof["limiter"] = ("neither roof: FP64 issue and latency at 24 of 64 warps per SM on "
+                           "the y and z sweeps (profiles/pencil_stage_traffic_jet128x64x64.md)")
 
     cpu = None
     if not args.no_cpu:
@@ -832,7 +835,7 @@ def main() -> int:
                    "serial_one_stream": e2e_serial},
            "gpu_launches": stages * launches_per_stage, **extras}
     print(json.dumps(out), flush=True)
-    if world > 1:
+    if distributed:
         dist.destroy_process_group()
     return 0
 
