@@ -298,7 +298,8 @@ def ensemble_record(f3d, dev, k: int, warm: int = 3, check_steps: int = 20) -> d
     tuned = [S.DeviceCase(c, device=dev, precision=1, tile="auto") for c in cases]
     modes = {}
     for mode, dcs, nst in (("graph", tuned, 16), ("graph_s32", tuned, 32),
-                           ("graph_pencil", pencil, 16), ("persistent", pencil, 16)):
+                           ("graph_pencil", pencil, 16), ("persistent", pencil, 16),
+                           ("hybrid", pencil, 16)):
         batch = B.Batch(dcs, device=dev, mode=mode.split("_")[0], streams=nst)
         batch.capture()
         for _ in range(warm):
@@ -316,9 +317,20 @@ def ensemble_record(f3d, dev, k: int, warm: int = 3, check_steps: int = 20) -> d
         batch.close()
     best = max(modes, key=lambda m: modes[m][0])
     value, ms, per_step = modes[best]
+
+    def persistent_launches(dcs):  # per step: two kernels per chunk and stage, four for law 2
+        groups = {}
+        for d in dcs:
+            key = (d.case.ns, d.transport.law == 2)
+            groups[key] = groups.get(key, 0) + 1
+        return 3 * sum(((n + 19) // 20) * (4 if law2 else 2) for (_, law2), n in groups.items())
+
+    small = [d for d in pencil if d.case.cells <= B.SMALL_CELLS]
     launches = (3 * sum(d.launches_per_stage() for d in tuned) if best in ("graph", "graph_s32")
                 else 3 * sum(d.launches_per_stage() for d in pencil) if best == "graph_pencil"
-                else 3 * 4 * len({c.ns for c in cases}))
+                else persistent_launches(pencil) if best == "persistent"
+                else persistent_launches(small)
+                + 3 * sum(d.launches_per_stage() for d in pencil if d.case.cells > B.SMALL_CELLS))
     del pencil, tuned
     torch.cuda.empty_cache()
     # bounded error check

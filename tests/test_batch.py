@@ -21,7 +21,7 @@ def _state(dc):
     return U, Q, r
 
 
-MODES = ["persistent", "graph"]
+MODES = ["persistent", "graph", "hybrid"]
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -278,3 +278,41 @@ def test_persistent_wait_runs_out_and_reports(f3d, cuda_ok):
                 assert np.linalg.norm((a[k] - c[k]).ravel()) <= 1e-12 * n
     b.close()
     b2.close()
+
+
+def test_hybrid_batch_splits_the_cases(f3d, oracle, cuda_ok):
+    """Hybrid mode with the size limit between the mix's cases: the cases of at most 12^3
+    cells run in the persistent part, the others in the graph part, both in one CUDA graph per
+    step.  After two captured steps every case is within 1e-12 of the oracle, and the graph
+    part's cases are bit for bit where they end when run alone."""
+    S = f3d.solver_module()
+    B = f3d.batch_module()
+    cases = _mix(f3d)
+    dcs = [S.DeviceCase(c, tile=3) for c in cases]
+    b = B.Batch(dcs, mode="hybrid", small_cells=12 ** 3)
+    assert [p.mode for p in b.parts] == ["persistent", "graph"]
+    big = [dc for dc in b.parts[1].cases]
+    assert all(dc.case.cells > 12 ** 3 for dc in big)
+    assert all(dc.case.cells <= 12 ** 3 for dc in b.parts[0].cases)
+    alone = {id(dc): S.DeviceCase(dc.case, tile=3) for dc in big}
+    ocs = [oracle.OracleCase(c) for c in cases]
+    b.capture()
+    for _ in range(2):
+        b.step()
+        for oc in ocs:
+            oc.step()
+        for a in alone.values():
+            a.step()
+    b.status()
+    I = oracle.interior
+    for dc, oc, c in zip(dcs, ocs, cases):
+        U = dc.conserved()
+        mom = np.linalg.norm(I(oc.U[1:4]).ravel())
+        for n in range(5):
+            ref = I(oc.U[n])
+            scale = mom if 1 <= n <= 3 else np.linalg.norm(ref.ravel())
+            assert np.linalg.norm((I(U[n]) - ref).ravel()) / scale <= 1e-12, (c.name, n)
+    for dc in big:
+        for x, y in zip(_state(dc), _state(alone[id(dc)])):
+            assert np.array_equal(x, y), dc.case.name
+    b.close()
